@@ -1,0 +1,362 @@
+"""SpMM throughput of the B200 FlashMatrix drop-in on synthetic R-MAT.
+
+Workload (one step = one SpMM over the whole matrix): R-MAT scale 24
+(16,777,216 vertices, edge factor 16, a/b/c/d = 0.57/0.19/0.19/0.05, seed 1,
+vertex labels permuted, duplicates and self-loops removed, unweighted) in the
+2D tile format, times a dense FP32 n x 16 matrix with N(0,1) entries.
+
+Metric: GB/s of algorithmic traffic per SpMM,
+    B_alg = 4 (n_rows + 1) + 4 nnz (1 + weighted) + n_cols k s + n_rows k s,
+divided by the device time (CUDA events, max over ranks).  Inputs (X 1.07 GB,
+column indices ~1 GB) are larger than the 126 MB L2, so no flush is needed.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl fmx|reference]
+      [--scale 24 --k 16 --weighted]
+
+--impl reference times the reference's CPU SpMM algorithm (the oracle's C
+restatement of FlashMatrix's 2D traversal; the reference library itself
+cannot be built here) on all host cores over a bounded sample of block rows.
+Under torchrun every rank runs an independent replica (the path does not
+need a data exchange); value = all ranks' bytes / max rank time.
+"""
+import argparse
+import datetime
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=2000)
+    p.add_argument("--warmup", type=int, default=20)
+    p.add_argument("--impl", default="fmx", choices=["fmx", "reference"])
+    p.add_argument("--scale", type=int, default=24)
+    p.add_argument("--k", type=int, default=16)
+    p.add_argument("--weighted", action="store_true")
+    p.add_argument("--no-permute", action="store_true")
+    p.add_argument("--block", type=int, default=16384)
+    p.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample time")
+    p.add_argument("--e2e-steps", type=int, default=5)
+    p.add_argument("--skip-cpu", action="store_true")
+    return p.parse_args()
+
+
+def workload_name(a):
+    return (f"rmat-s{a.scale}-ef16-k{a.k}-f32-{'weighted' if a.weighted else 'unweighted'}"
+            f"{'' if a.no_permute else '-permuted'}")
+
+
+def build_graph(a):
+    from flashx_b200 import matrix_image
+    from flashx_b200.graphs import rmat_edges
+    t0 = time.time()
+    src, dst = rmat_edges(a.scale, seed=1, permute=not a.no_permute)
+    vals = None
+    if a.weighted:
+        rng = np.random.default_rng(7)
+        vals = (1.0 - rng.random(len(src), dtype=np.float32)).astype(np.float32)  # (0, 1]
+    n = 1 << a.scale
+    img = matrix_image.build(src, dst, vals, nrows=n, ncols=n, block_size=(a.block, a.block), dedup=True)
+    del src, dst, vals
+    return img, time.time() - t0
+
+
+def b_alg(n_rows, n_cols, nnz, k, weighted, s=4):
+    return 4 * (n_rows + 1) + 4 * nnz * (1 + int(weighted)) + n_cols * k * s + n_rows * k * s
+
+
+def cpu_info():
+    model = ""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return os.cpu_count() or 1, model
+
+
+def cpu_sample(img, a, nthreads, target_s, reps=None):
+    """Time the oracle (the reference's CPU SpMM algorithm) on the first block
+    rows of the image holding ~target_s seconds of work; returns GB/s scaled to
+    the full matrix's B_alg per nnz, plus a description of the sample."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    idx, mat = img.bytes()
+    inf = img.info()
+    nb = oracle.num_block_rows(idx)
+    rng = np.random.default_rng(3)
+    X = rng.standard_normal((inf["ncols"], a.k)).astype(np.float32)
+    # calibrate on one block row, then grow the sample to the target time
+    b1 = 1
+    t = time.perf_counter()
+    oracle.spmm(idx, mat, X, nthreads=nthreads, brows=(0, b1))
+    dt = max(time.perf_counter() - t, 1e-4)
+    b1 = int(min(nb, max(1, target_s / dt)))
+    nnz_s = oracle.block_rows_nnz(idx, mat, 0, b1)
+    times = []
+    for _ in range(reps or 1):
+        t = time.perf_counter()
+        oracle.spmm(idx, mat, X, nthreads=nthreads, brows=(0, b1))
+        times.append(time.perf_counter() - t)
+    full = b_alg(inf["nrows"], inf["ncols"], inf["nnz"], a.k, a.weighted)
+    per_nnz = full / inf["nnz"]
+    gbs = [per_nnz * nnz_s / x / 1e9 for x in times]
+    sample = (f"block rows [0,{b1}) of {nb} ({nnz_s} of {inf['nnz']} non-zeros, "
+              f"{a.block}x{a.block} tiles), FP32 k={a.k}, {nthreads} threads, "
+              f"GB/s = B_alg per nnz x sample nnz / time")
+    return gbs, sample, times
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.gpu)],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < 5:
+                time.sleep(0.05)
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def read_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def read_traffic(name):
+    """Per-launch DRAM bytes of the SpMM kernel from a committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", f"{name}.traffic.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return d
+    except (OSError, ValueError):
+        return None
+
+
+def run_reference(a, rank, world):
+    if rank != 0:
+        return
+    img, build_s = build_graph(a)
+    nthreads, model = cpu_info()
+    inf = img.info()
+    per = max(a.cpu_seconds / max(a.steps, 1), 0.5)
+    warm = min(a.warmup, 1)
+    for _ in range(warm):
+        cpu_sample(img, a, nthreads, per)
+    gbs, sample, times = cpu_sample(img, a, nthreads, per, reps=a.steps)
+    value = float(np.median(gbs))
+    line = {
+        "metric": "SpMM GB/s (algorithmic bytes / time)", "value": round(value, 3), "unit": "GB/s",
+        "impl": "reference", "n_gpus": world, "steps": a.steps, "warmup": warm,
+        "ms_per_step": round(float(np.median(times)) * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": workload_name(a), "scale": a.scale, "k": a.k, "nnz": inf["nnz"],
+                   "block": a.block, "sample": sample},
+        "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": nthreads, "kind": "port",
+                         "sample": sample + f"; CPU: {model}"},
+        "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    a = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.impl == "reference":
+        return run_reference(a, rank, world)
+
+    import torch
+    import torch.distributed as dist
+    from flashx_b200 import sparse_matrix
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=dev)
+
+    img, build_s = build_graph(a)
+    inf = img.info()
+    t0 = time.time()
+    m = sparse_matrix.create(img, None, device=local)
+    create_s = time.time() - t0
+    n_rows, n_cols, nnz, k = inf["nrows"], inf["ncols"], inf["nnz"], a.k
+    light, tasks, heavy, kernels = m.schedule()
+    cpu_img = img if (rank == 0 and world == 1 and not a.skip_cpu) else None
+    if cpu_img is None:
+        del img
+
+    g = torch.Generator(device=dev)
+    g.manual_seed(1234 + rank)
+    X = torch.randn((n_cols, k), generator=g, device=dev, dtype=torch.float32)
+    Y = torch.empty((n_rows, k), device=dev, dtype=torch.float32)
+    stream = torch.cuda.current_stream(dev)
+    st = stream.cuda_stream
+
+    def step():
+        if not m.multiply(X, Y, stream=st):
+            raise RuntimeError("fmx_spmm failed")
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+
+    # -- timed region --
+    clocks = ClockSampler(local)
+    clocks.start()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    t_begin = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_begin.record(stream)
+    for i in range(a.steps):
+        starts[i].record(stream)
+        step()
+        ends[i].record(stream)
+    t_end.record(stream)
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    total_ms = t_begin.elapsed_time(t_end)
+    launch_ms = float(np.mean([s.elapsed_time(e) for s, e in zip(starts, ends)]))
+    if world > 1:
+        tt = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_ms = float(tt.item())
+
+    per_spmm = b_alg(n_rows, n_cols, nnz, k, a.weighted)
+    value = per_spmm * a.steps * world / (total_ms / 1e3) / 1e9
+    peak, peak_kind = read_peaks()
+    achieved = per_spmm / (launch_ms / 1e3) / 1e9
+    tr = read_traffic(workload_name(a))
+    traffic = None
+    if tr is not None:
+        traffic = tr.get("bytes_per_launch")
+
+    # -- end to end through the C ABI with host buffers (pinned) --
+    e2e = None
+    if a.e2e_steps > 0:
+        Xh = torch.empty((n_cols, k), dtype=torch.float32, pin_memory=True)
+        Xh.copy_(X.cpu())
+        Yh = torch.empty((n_rows, k), dtype=torch.float32, pin_memory=True)
+        Xn, Yn = Xh.numpy(), Yh.numpy()
+        m.multiply_host(Xn, Yn)   # warm-up: staging buffers
+        if world > 1:
+            dist.barrier()
+        t = time.perf_counter()
+        for _ in range(a.e2e_steps):
+            m.multiply_host(Xn, Yn)
+        e2e_s = time.perf_counter() - t
+        if world > 1:
+            tt = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            e2e_s = float(tt.item())
+        e2e = {"value": round(per_spmm * a.e2e_steps * world / e2e_s / 1e9, 3), "unit": "GB/s",
+               "h2d_bytes_per_step": n_cols * k * 4, "d2h_bytes_per_step": n_rows * k * 4,
+               "ms_per_step": round(e2e_s / a.e2e_steps * 1e3, 3)}
+
+    cpu = None
+    if cpu_img is not None:
+        nthreads, model = cpu_info()
+        gbs, sample, _ = cpu_sample(cpu_img, a, nthreads, a.cpu_seconds)
+        cpu = {"value": round(gbs[0], 3), "unit": "GB/s", "cores": nthreads, "kind": "port",
+               "sample": sample + f"; CPU: {model}"}
+
+    if rank == 0:
+        line = {
+            "metric": "SpMM GB/s (algorithmic bytes / time)",
+            "value": round(value, 3), "unit": "GB/s", "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": round(total_ms / a.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": workload_name(a), "scale": a.scale, "k": k, "edge_factor": 16,
+                       "abcd": [0.57, 0.19, 0.19, 0.05], "nnz": nnz, "n_rows": n_rows,
+                       "block": a.block, "bytes_alg_per_step": per_spmm,
+                       "l2": "no flush: X (%.2f GB) and indices (%.2f GB) exceed the 126 MB L2"
+                             % (n_cols * k * 4 / 1e9, nnz * 4 / 1e9),
+                       "parallelism": f"replicas{world}" if world > 1 else "single",
+                       "host_build_s": round(build_s, 2), "device_create_s": round(create_s, 2),
+                       "schedule": {"light_rows": light, "warp_tasks": tasks, "heavy_rows": heavy}},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                         "kernel": "spmm_kernel (+ spmm_fixup_kernel), per fmx_spmm call",
+                         "traffic": traffic},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": a.steps * kernels,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

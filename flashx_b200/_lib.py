@@ -1,0 +1,93 @@
+"""ctypes binding of libfmx.so (the C ABI declared in include/fmx.h).
+
+The library must exist (built in-tree by flashx_b200.build); there is no
+fallback implementation: importing this module without it raises.
+"""
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libfmx.so")
+
+FMX_OK = 0
+FMX_ERR_INVAL = -1
+FMX_ERR_DIM = -2
+FMX_ERR_TYPE = -3
+FMX_ERR_IMAGE = -4
+FMX_ERR_OOM = -5
+FMX_ERR_CUDA = -6
+FMX_ERR_IO = -7
+FMX_ERR_UNSUPPORTED = -8
+
+F32, F64, BF16, I32, I64 = 0, 1, 2, 3, 4
+P_BOOL, P_INTEGER, P_LONG, P_FLOAT, P_DOUBLE = 0, 4, 6, 8, 9
+
+BUILD_DEDUP = 0x1
+BUILD_KEEP_SELF_LOOPS = 0x2
+BUILD_REF_VALUE_LAYOUT = 0x4
+
+
+class FmxError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{msg} [status {code}]")
+        self.code = code
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `python flashx_b200/build.py` "
+            "(the CUDA library is required; there is no CPU fallback)")
+    return C.CDLL(LIB_PATH)
+
+
+lib = _load()
+
+_vp, _sz, _u64, _i64, _u32, _int, _d = C.c_void_p, C.c_size_t, C.c_uint64, C.c_int64, C.c_uint32, C.c_int, C.c_double
+_P = C.POINTER
+
+_SIGS = {
+    "fmx_strerror": (C.c_char_p, [_int]),
+    "fmx_last_error": (C.c_char_p, []),
+    "fmx_version": (C.c_char_p, []),
+    "fmx_image_build": (_int, [_vp, _vp, _vp, _int, _u64, _u64, _u64, _u32, _u32, _int, _int, _P(_vp)]),
+    "fmx_image_from_bytes": (_int, [_vp, _sz, _vp, _sz, _P(_vp)]),
+    "fmx_image_load": (_int, [C.c_char_p, C.c_char_p, _P(_vp)]),
+    "fmx_image_dump": (_int, [_vp, C.c_char_p, C.c_char_p]),
+    "fmx_image_bytes": (_int, [_vp, _P(_vp), _P(_sz), _P(_vp), _P(_sz)]),
+    "fmx_image_info": (_int, [_vp, _P(_u64), _P(_u64), _P(_u64), _P(_u32), _P(_int), _P(_u32), _P(_u32)]),
+    "fmx_image_verify": (_int, [_vp]),
+    "fmx_image_free": (_int, [_vp]),
+    "fmx_matrix_create": (_int, [_vp, _vp, _int, _P(_vp)]),
+    "fmx_matrix_load": (_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, _int, _P(_vp)]),
+    "fmx_matrix_info": (_int, [_vp, _P(_u64), _P(_u64), _P(_u64), _P(_int), _P(_int)]),
+    "fmx_matrix_device_bytes": (_int, [_vp, _P(_u64)]),
+    "fmx_matrix_transpose": (_int, [_vp, _P(_vp)]),
+    "fmx_matrix_free": (_int, [_vp]),
+    "fmx_spmm": (_int, [_vp, _int, _vp, _i64, _int, _vp, _i64, _i64, _vp, _vp, _vp]),
+    "fmx_spmm_host": (_int, [_vp, _int, _vp, _i64, _int, _vp, _i64, _i64]),
+    "fmx_matrix_schedule": (_int, [_vp, _P(_u64), _P(_u64), _P(_u64), _P(_u64)]),
+    "fmx_rmat_edges_host": (_int, [_int, _u64, _d, _d, _d, _u64, _int, _vp, _vp, _int]),
+    "fmx_rmat_edges_device": (_int, [_int, _u64, _d, _d, _d, _u64, _int, _vp, _vp, _vp]),
+}
+
+for _name, (_res, _args) in _SIGS.items():
+    _f = getattr(lib, _name)
+    _f.restype = _res
+    _f.argtypes = _args
+
+
+def last_error():
+    s = lib.fmx_last_error()
+    return s.decode() if s else ""
+
+
+def check(code):
+    """Raise FmxError for a non-zero status of a C-ABI call."""
+    if code != FMX_OK:
+        raise FmxError(code, last_error() or lib.fmx_strerror(code).decode())
+    return code
+
+
+def exported_symbols():
+    return list(_SIGS)

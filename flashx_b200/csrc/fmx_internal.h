@@ -1,0 +1,93 @@
+// Internal declarations shared by the host (C++) and device (CUDA) halves of
+// libfmx.  Not installed; the public surface is include/fmx.h.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <memory>
+#include <atomic>
+
+#include "../../include/fmx.h"
+
+namespace fmx {
+
+// ---- error reporting ------------------------------------------------------
+// Sets the thread-local message returned by fmx_last_error() and returns code.
+int set_error(int code, const char *fmt, ...);
+
+// ---- the reference's on-disk 2D format -------------------------------------
+// matrix_header::info (matrix/matrix_header.h:102-121), x86-64 layout,
+// padded to one 4096-byte page.
+constexpr size_t kPage = 4096;
+constexpr int64_t kMagic = 0x123456789FFFFFFLL;
+constexpr int kVersion = 2;
+constexpr int kSparse = 2;    // matrix_type::SPARSE
+constexpr int kRow2D = 2;     // matrix_layout_t::L_ROW_2D
+constexpr uint32_t kMaxBlock = 32768;  // block_max_num_rows/cols (matrix_header.h:42-43)
+
+struct header_info {
+	int64_t magic_number;
+	int32_t version_number;
+	int32_t type;
+	uint64_t entry_size;
+	uint64_t nrows;
+	uint64_t ncols;
+	int32_t layout;
+	int32_t data_type;
+	uint64_t block_2d_height;
+	uint64_t block_2d_width;
+};
+static_assert(sizeof(header_info) == 64, "matrix_header field layout");
+
+// sparse_block_2d header (matrix/sparse_matrix_format.h:215-224).
+struct tile_header {
+	uint32_t brow, bcol, nnz;
+	uint16_t nrow, ncoo;
+};
+static_assert(sizeof(tile_header) == 16, "sparse_block_2d is 16 bytes");
+
+inline size_t tile_bytes(const tile_header &t, size_t esize) {
+	return sizeof(tile_header) + size_t(t.nrow) * 2 + size_t(t.nnz) * 2 + 2 + esize * t.nnz;
+}
+inline size_t tile_rheader(const tile_header &t) {
+	return size_t(t.nrow - t.ncoo) * 2 + size_t(t.nnz - t.ncoo) * 2 + 2;
+}
+
+size_t prim_size(int prim);   // 0 for bool, -1 (SIZE_MAX) for unknown
+bool is_pow2(uint64_t v);
+
+// A host image: owns the .mat_idx and .mat bytes.
+struct image {
+	std::vector<char> idx;
+	std::vector<char> mat;
+	header_info h{};
+	uint64_t nbrows = 0;
+	uint64_t nnz = 0;          // filled by validate()
+	const int64_t *offs() const { return reinterpret_cast<const int64_t *>(idx.data() + kPage); }
+};
+
+// Check the header pair, the index and every tile's bounds; counts nnz.
+int validate(image &img, bool deep);
+
+// Host CSR decoded from an image: rows ascending, columns in the order the
+// reference visits them (ascending block column, then ascending column).
+struct host_csr {
+	uint64_t nrows = 0, ncols = 0, nnz = 0;
+	int prim = 0;              // entry prim type (FMX_P_*)
+	size_t esize = 0;          // entry bytes (0 = binary)
+	std::vector<uint32_t> row_ptr;   // nrows + 1 (nnz < 2^32 enforced)
+	std::vector<int32_t> col;
+	std::vector<char> val;     // nnz * esize bytes
+};
+int decode_to_csr(const image &img, host_csr &out, int nthreads);
+
+int default_threads();
+
+} // namespace fmx
+
+struct fmx_image {
+	fmx::image im;
+};

@@ -1,0 +1,178 @@
+/*
+ * fmx.h -- C ABI of the B200 FlashMatrix SpMM library (libfmx.so).
+ *
+ * Plain C types only: pointers, sizes, integer codes.  Device pointers are
+ * CUDA device addresses on the matrix's device; `stream` is a cudaStream_t
+ * passed as void* (NULL = the legacy default stream).
+ *
+ * Every function returns 0 (FMX_OK) or a negative fmx_status.  The text of
+ * the last failure on the calling thread is returned by fmx_last_error().
+ *
+ * Reference interfaces replaced (paths relative to the FlashX tree):
+ *   matrix/sparse_matrix_format.h:441-532   SpM_2d_index / SpM_2d_storage
+ *   matrix/sparse_matrix.h:522-539,679-707  sparse_matrix::create
+ *   matrix/sparse_matrix.h:629-650          sparse_matrix::multiply
+ *   matrix/fm_utils.cpp:617-841             create_2d_matrix (format builder)
+ */
+#ifndef FMX_H
+#define FMX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+enum fmx_status {
+	FMX_OK = 0,
+	FMX_ERR_INVAL = -1,      /* null pointer, bad flag, bad argument          */
+	FMX_ERR_DIM = -2,        /* incompatible dimensions (sparse_matrix.cpp:712-718) */
+	FMX_ERR_TYPE = -3,       /* unsupported or mismatched types (:754-766)    */
+	FMX_ERR_IMAGE = -4,      /* malformed .mat / .mat_idx image               */
+	FMX_ERR_OOM = -5,        /* host or device allocation failed              */
+	FMX_ERR_CUDA = -6,       /* a CUDA runtime call failed                    */
+	FMX_ERR_IO = -7,         /* file could not be opened / read / written     */
+	FMX_ERR_UNSUPPORTED = -8 /* valid request this build does not implement   */
+};
+
+/* ---- element types ----------------------------------------------------- */
+/* Dense operand types.  The numbering is this library's own. */
+enum fmx_dtype {
+	FMX_F32 = 0,
+	FMX_F64 = 1,
+	FMX_BF16 = 2, /* input only; accumulates and writes FP32 or BF16 */
+	FMX_I32 = 3,
+	FMX_I64 = 4
+};
+
+/* Sparse entry types stored in the image header (matrix/generic_type.h:57-70
+ * prim_type order: P_BOOL=0 .. P_FLOAT=8, P_DOUBLE=9). */
+enum fmx_prim_type {
+	FMX_P_BOOL = 0,
+	FMX_P_INTEGER = 4,
+	FMX_P_LONG = 6,
+	FMX_P_FLOAT = 8,
+	FMX_P_DOUBLE = 9
+};
+
+typedef struct fmx_matrix fmx_matrix; /* a matrix resident on one GPU */
+typedef struct fmx_image fmx_image;   /* a host-side .mat/.mat_idx pair  */
+
+const char *fmx_strerror(int status);
+const char *fmx_last_error(void);
+/* Library version string, e.g. "fmx 0.1 sm_100a". */
+const char *fmx_version(void);
+
+/* ---- matrix images (host) ------------------------------------------------
+ * A matrix image is the reference's on-disk 2D format: a 4096-byte
+ * matrix_header page followed by block rows of packed sparse_block_2d tiles
+ * (.mat), plus an index of header + (nbrows+1) int64 byte offsets (.mat_idx).
+ * Replaces SpM_2d_index::load / SpM_2d_storage::load
+ * (matrix/sparse_matrix_format.cpp:238-306) and ::dump (:164-181,417-420).
+ */
+
+/* Builder flags (matrix/fm_utils.cpp:37-49, 444-482). */
+#define FMX_BUILD_DEDUP 0x1          /* set_deduplicate(true)                  */
+#define FMX_BUILD_KEEP_SELF_LOOPS 0x2 /* set_remove_self_edge(false)            */
+#define FMX_BUILD_REF_VALUE_LAYOUT 0x4 /* place tile values the way the reference
+                                         builder does (fm_utils.cpp:240-241,259-260
+                                         copy each tile's values from the start of
+                                         the row); default keeps each entry's own value */
+
+/* Build an image from an edge list (src[i] -> dst[i], optional values of
+ * `val_type` (FMX_P_BOOL = no values, FMX_P_FLOAT, FMX_P_DOUBLE, FMX_P_INTEGER,
+ * FMX_P_LONG)).  nrows/ncols = 0 means max id + 1 (fm_utils.cpp:730-739,788).
+ * block_h/block_w: powers of two <= 32768 (matrix_header.h:42-62).
+ * Replaces fm::create_2d_matrix (matrix/fm_utils.cpp:617-715,726-841). */
+int fmx_image_build(const uint32_t *src, const uint32_t *dst, const void *vals,
+                    int val_type, uint64_t nedges, uint64_t nrows, uint64_t ncols,
+                    uint32_t block_h, uint32_t block_w, int flags, int nthreads,
+                    fmx_image **out);
+/* Wrap copies of an existing .mat_idx / .mat byte pair (validated). */
+int fmx_image_from_bytes(const void *idx, size_t idx_len, const void *mat,
+                         size_t mat_len, fmx_image **out);
+int fmx_image_load(const char *mat_idx_path, const char *mat_path, fmx_image **out);
+int fmx_image_dump(const fmx_image *img, const char *mat_idx_path, const char *mat_path);
+/* Borrow the bytes of an image (valid until fmx_image_free). */
+int fmx_image_bytes(const fmx_image *img, const void **idx, size_t *idx_len,
+                    const void **mat, size_t *mat_len);
+/* nrows, ncols, nnz, entry size in bytes (0 = binary), prim type, block h, w. */
+int fmx_image_info(const fmx_image *img, uint64_t *nrows, uint64_t *ncols,
+                   uint64_t *nnz, uint32_t *entry_size, int *prim_type,
+                   uint32_t *block_h, uint32_t *block_w);
+/* Check every tile invariant (sparse_matrix_format.cpp:36-60,371-415). */
+int fmx_image_verify(const fmx_image *img);
+int fmx_image_free(fmx_image *img);
+
+/* ---- GPU-resident matrices ------------------------------------------------
+ * Replaces sparse_matrix::create(SpM_2d_index::ptr, SpM_2d_storage::ptr[,
+ * t_index, t_storage]) (matrix/sparse_matrix.cpp:679-707).  The image is
+ * decoded on the host and its tiles are kept resident in HBM of `device`
+ * with int32 column indices.  `t_img` (nullable) is the transpose image of an
+ * asymmetric matrix (block_sparse_asym_matrix, sparse_matrix.cpp:582-665).
+ */
+int fmx_matrix_create(const fmx_image *img, const fmx_image *t_img, int device,
+                      fmx_matrix **out);
+/* Convenience: fmx_image_load + fmx_matrix_create (+ free of the images). */
+int fmx_matrix_load(const char *mat_idx_path, const char *mat_path,
+                    const char *t_mat_idx_path, const char *t_mat_path,
+                    int device, fmx_matrix **out);
+int fmx_matrix_info(const fmx_matrix *m, uint64_t *nrows, uint64_t *ncols,
+                    uint64_t *nnz, int *prim_type, int *symmetric);
+/* Device bytes held by the matrix (tiles, schedule, scratch). */
+int fmx_matrix_device_bytes(const fmx_matrix *m, uint64_t *bytes);
+/* sparse_matrix::transpose (sparse_matrix.cpp:514-516,619-626): a symmetric
+ * matrix returns itself; an asymmetric pair swaps its two images.  The
+ * returned handle shares device memory with `m` and must be freed with
+ * fmx_matrix_free before or after `m`. */
+int fmx_matrix_transpose(const fmx_matrix *m, fmx_matrix **out);
+int fmx_matrix_free(fmx_matrix *m);
+
+/* ---- SpMM -----------------------------------------------------------------
+ * Y = diag(row_scale_out) * A * diag(row_scale_in) * X   (scales nullable)
+ * Replaces sparse_matrix::multiply(in, out) (matrix/sparse_matrix.cpp:709-771)
+ * and the spmm_creator<DenseType, SparseType> tasks (sparse_matrix.h:219-436).
+ *   X: ncols x k, row-major, leading dimension ldx (elements), type x_type
+ *   Y: nrows x k, row-major, leading dimension ldy, type y_type; fully
+ *      overwritten (block_spmm_task::notify_complete, sparse_matrix.cpp:354-393)
+ *   Supported (x_type -> y_type): F32->F32, F64->F64, BF16->F32, BF16->BF16,
+ *   I32->I32, I64->I64.  A binary matrix multiplies by 1; a weighted matrix's
+ *   entries are converted to the accumulation type (float entries with F64
+ *   operands reproduce spmm_creator<double,float>, test-eigen.cpp:47).
+ *   Scales have the accumulation type (float for F32/BF16, double for F64).
+ * Each output row is summed in ascending column order by one lane group, the
+ * reference's order, except rows longer than the split threshold, which are
+ * summed as fixed-order partial chunks.  Asynchronous on `stream`. */
+int fmx_spmm(const fmx_matrix *m, int x_type, const void *X, int64_t ldx,
+             int y_type, void *Y, int64_t ldy, int64_t k,
+             const void *row_scale_in, const void *row_scale_out, void *stream);
+
+/* Host-buffer SpMM: copies X in and Y out through the device (pinned or
+ * pageable host memory), synchronous.  The e2e path a CPU caller uses. */
+int fmx_spmm_host(const fmx_matrix *m, int x_type, const void *X_host, int64_t ldx,
+                  int y_type, void *Y_host, int64_t ldy, int64_t k);
+
+/* Work decomposition of the resident matrix: rows summed by one lane group,
+ * warp tasks (long rows and chunks of very long rows), rows finished by the
+ * chunk-sum pass, and kernel launches per 128-column panel of one fmx_spmm. */
+int fmx_matrix_schedule(const fmx_matrix *m, uint64_t *n_light_rows, uint64_t *n_split_tasks,
+                        uint64_t *n_heavy_rows, uint64_t *kernels_per_spmm);
+
+/* ---- synthetic graphs ---------------------------------------------------------
+ * R-MAT edges (a,b,c; d = 1-a-b-c) of 2^scale vertices, counter-based so the
+ * host and device streams are identical.  `permute` relabels vertices by a
+ * seeded bijection (Boost rmat_iterator permute_vertices, used by
+ * flash-graph/tools/rmat-gen.cpp:43-44). */
+int fmx_rmat_edges_host(int scale, uint64_t nedges, double a, double b, double c,
+                        uint64_t seed, int permute, uint32_t *src, uint32_t *dst,
+                        int nthreads);
+int fmx_rmat_edges_device(int scale, uint64_t nedges, double a, double b, double c,
+                          uint64_t seed, int permute, uint32_t *src_dev,
+                          uint32_t *dst_dev, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FMX_H */

@@ -1,0 +1,208 @@
+"""ctypes wrapper of the CPU ORACLE (test infrastructure only).
+
+Loaded only by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline
+and reference legs -- never by the flashx_b200 package.
+
+  liboracle.so       oracle/fmx_oracle.c, the C restatement of the reference's
+                     builder, SpMM traversal and PageRank (built by `make -C oracle`).
+  libfmx_refwalk.so  oracle/ref_walk.cpp compiled against the reference's own
+                     tile headers in place (`make -C oracle ref`, only where the
+                     reference tree exists); optional.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "_build", "liboracle.so")
+REFWALK_SO = os.path.join(HERE, "_ref", "libfmx_refwalk.so")
+REFERENCE_TREE = "/root/reference"
+
+D_F32, D_F64, D_I32, D_I64 = 0, 1, 3, 4
+P_BOOL, P_INTEGER, P_LONG, P_FLOAT, P_DOUBLE = 0, 4, 6, 8, 9
+_NP = {D_F32: np.float32, D_F64: np.float64, D_I32: np.int32, D_I64: np.int64}
+_D_OF = {np.dtype(v): k for k, v in _NP.items()}
+
+
+def build(ref=None):
+    """Compile the oracle (and the reference walker when the tree exists)."""
+    subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
+    if ref is None:
+        ref = os.path.isdir(os.path.join(REFERENCE_TREE, "matrix"))
+    if ref:
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REFERENCE_TREE}"], check=True)
+
+
+_orc = None
+_ref = None
+
+
+def orc():
+    global _orc
+    if _orc is None:
+        if not os.path.exists(ORACLE_SO):
+            build(ref=False)
+        L = C.CDLL(ORACLE_SO)
+        vp, sz, u64, i64, i32 = C.c_void_p, C.c_size_t, C.c_uint64, C.c_int64, C.c_int
+        L.orc_build_image.restype = i32
+        L.orc_build_image.argtypes = [vp, vp, vp, i32, u64, u64, u64, C.c_uint32, C.c_uint32, i32, i32, i32,
+                                      C.POINTER(vp), C.POINTER(sz), C.POINTER(vp), C.POINTER(sz)]
+        L.orc_free.argtypes = [vp]
+        L.orc_nonzeros.restype = i64
+        L.orc_nonzeros.argtypes = [vp, sz, vp, sz, vp, vp, u64]
+        L.orc_spmm.restype = i32
+        L.orc_spmm.argtypes = [vp, sz, vp, sz, i32, vp, vp, u64, i32, i32, u64, i32, u64, u64]
+        L.orc_num_block_rows.restype = i64
+        L.orc_num_block_rows.argtypes = [vp, sz]
+        L.orc_block_rows_nnz.restype = i64
+        L.orc_block_rows_nnz.argtypes = [vp, sz, vp, sz, u64, u64]
+        L.orc_verify.restype = i32
+        L.orc_verify.argtypes = [vp, sz, vp, sz]
+        L.orc_pagerank.restype = i32
+        L.orc_pagerank.argtypes = [vp, sz, vp, sz, vp, sz, vp, sz, u64, C.c_float, i32, vp, C.POINTER(u64)]
+        L.orc_hilbert_xy2d.restype = i32
+        L.orc_hilbert_xy2d.argtypes = [i32, i32, i32]
+        L.orc_now.restype = C.c_double
+        _orc = L
+    return _orc
+
+
+def ref_available():
+    return os.path.exists(REFWALK_SO)
+
+
+def ref():
+    global _ref
+    if _ref is None:
+        if not os.path.exists(REFWALK_SO):
+            return None
+        L = C.CDLL(REFWALK_SO)
+        vp, u64, i64, i32 = C.c_void_p, C.c_uint64, C.c_int64, C.c_int
+        L.ref_spmm.restype = i32
+        L.ref_spmm.argtypes = [vp, vp, i32, vp, vp, u64]
+        L.ref_nonzeros.restype = i64
+        L.ref_nonzeros.argtypes = [vp, vp, vp, vp, u64]
+        L.ref_hilbert_xy2d.restype = i32
+        L.ref_hilbert_xy2d.argtypes = [i32, i32, i32]
+        L.ref_header.restype = i32
+        L.ref_header.argtypes = [vp] + [C.POINTER(u64)] * 5 + [C.POINTER(i32)] * 3
+        _ref = L
+    return _ref
+
+
+def build_image(src, dst, vals=None, nrows=0, ncols=0, block=(16384, 16384), dedup=False,
+                keep_self=False, ref_value_layout=False):
+    """Oracle builder -> (idx bytes, mat bytes)."""
+    src = np.ascontiguousarray(src, dtype=np.uint32)
+    dst = np.ascontiguousarray(dst, dtype=np.uint32)
+    prim, vp = P_BOOL, None
+    if vals is not None:
+        vals = np.ascontiguousarray(vals)
+        prim = {np.dtype(np.float32): P_FLOAT, np.dtype(np.float64): P_DOUBLE,
+                np.dtype(np.int32): P_INTEGER, np.dtype(np.int64): P_LONG}[vals.dtype]
+        vp = vals.ctypes.data
+    ip, il, mp, ml = C.c_void_p(), C.c_size_t(), C.c_void_p(), C.c_size_t()
+    rc = orc().orc_build_image(src.ctypes.data, dst.ctypes.data, vp, prim, len(src), nrows, ncols,
+                               block[0], block[1], int(dedup), int(keep_self), int(ref_value_layout),
+                               C.byref(ip), C.byref(il), C.byref(mp), C.byref(ml))
+    if rc:
+        raise ValueError("oracle builder rejected the edge list")
+    idx = C.string_at(ip, il.value)
+    mat = C.string_at(mp, ml.value)
+    orc().orc_free(ip)
+    orc().orc_free(mp)
+    return idx, mat
+
+
+def nonzeros(idx, mat):
+    n = orc().orc_nonzeros(idx, len(idx), mat, len(mat), None, None, 0)
+    if n < 0:
+        raise ValueError("malformed image")
+    r = np.empty(n, dtype=np.uint64)
+    c = np.empty(n, dtype=np.uint64)
+    orc().orc_nonzeros(idx, len(idx), mat, len(mat), r.ctypes.data, c.ctypes.data, n)
+    return r, c
+
+
+def header(idx):
+    h = np.frombuffer(idx[:64], dtype=np.uint8)
+    nrows = int(np.frombuffer(idx[24:32], dtype=np.uint64)[0])
+    ncols = int(np.frombuffer(idx[32:40], dtype=np.uint64)[0])
+    esize = int(np.frombuffer(idx[16:24], dtype=np.uint64)[0])
+    prim = int(np.frombuffer(idx[44:48], dtype=np.int32)[0])
+    bh = int(np.frombuffer(idx[48:56], dtype=np.uint64)[0])
+    bw = int(np.frombuffer(idx[56:64], dtype=np.uint64)[0])
+    del h
+    return dict(nrows=nrows, ncols=ncols, entry_size=esize, prim=prim, block_h=bh, block_w=bw)
+
+
+def spmm(idx, mat, X, nthreads=1, hilbert=False, cpu_cache_size=0, copy_task=True, brows=None):
+    """Oracle SpMM Y = A X (X: 2-D numpy array, ncols x k, row-major)."""
+    X = np.ascontiguousarray(X)
+    if X.ndim == 1:
+        X = X[:, None]
+    d = _D_OF[X.dtype]
+    h = header(idx)
+    Y = np.zeros((h["nrows"], X.shape[1]), dtype=X.dtype)
+    b0, b1 = (0, 0) if brows is None else brows
+    rc = orc().orc_spmm(idx, len(idx), mat, len(mat), d, X.ctypes.data, Y.ctypes.data, X.shape[1],
+                        nthreads, int(hilbert), cpu_cache_size, int(copy_task), b0, b1)
+    if rc:
+        raise ValueError("oracle SpMM failed")
+    return Y
+
+
+def ref_spmm(idx, mat, X, dense_double_sparse_float=False):
+    """SpMM through the reference's own tile iterators (None if not built)."""
+    L = ref()
+    if L is None:
+        return None
+    X = np.ascontiguousarray(X)
+    if X.ndim == 1:
+        X = X[:, None]
+    d = 5 if dense_double_sparse_float else _D_OF[X.dtype]
+    h = header(idx)
+    Y = np.zeros((h["nrows"], X.shape[1]), dtype=X.dtype)
+    if L.ref_spmm(idx, mat, d, X.ctypes.data, Y.ctypes.data, X.shape[1]):
+        raise ValueError("reference walk failed")
+    return Y
+
+
+def ref_nonzeros(idx, mat):
+    L = ref()
+    if L is None:
+        return None
+    n = L.ref_nonzeros(idx, mat, None, None, 0)
+    r = np.empty(n, dtype=np.uint64)
+    c = np.empty(n, dtype=np.uint64)
+    L.ref_nonzeros(idx, mat, r.ctypes.data, c.ctypes.data, n)
+    return r, c
+
+
+def verify(idx, mat):
+    return orc().orc_verify(idx, len(idx), mat, len(mat))
+
+
+def pagerank(idx, mat, t_idx, t_mat, max_iters=30, damping=0.85, nthreads=1):
+    n = header(idx)["nrows"]
+    pr = np.empty(n, dtype=np.float32)
+    it = C.c_uint64()
+    rc = orc().orc_pagerank(idx, len(idx), mat, len(mat), t_idx, len(t_idx), t_mat, len(t_mat), max_iters,
+                            damping, nthreads, pr.ctypes.data, C.byref(it))
+    if rc:
+        raise ValueError("oracle PageRank failed")
+    return pr, it.value
+
+
+def num_block_rows(idx):
+    return orc().orc_num_block_rows(idx, len(idx))
+
+
+def block_rows_nnz(idx, mat, b0, b1):
+    return orc().orc_block_rows_nnz(idx, len(idx), mat, len(mat), b0, b1)
+
+
+def now():
+    return orc().orc_now()

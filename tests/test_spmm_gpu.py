@@ -1,0 +1,210 @@
+"""GPU parity: libfmx's CUDA SpMM against the CPU oracle on the same image.
+
+Bar: bit-exact for integer types and for every row summed by one lane group
+(rows of <= 512 entries are summed in the reference's ascending-column order
+with separate multiply and add roundings); bit-exact for split rows when the
+inputs are integer-valued (all partial sums exact); otherwise within
+RTOL = 1e-5 relative (FP32) of the oracle.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from flashx_b200 import _lib, matrix_image, sparse_matrix, create_2d_matrix
+from flashx_b200.graphs import rmat_edges
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-5
+
+
+def _graph(n, m, seed, heavy=()):
+    rng = np.random.default_rng(seed)
+    src = rng.integers(0, n, m).astype(np.uint32)
+    dst = rng.integers(0, n, m).astype(np.uint32)
+    extra_s, extra_d = [], []
+    for row, deg in heavy:
+        extra_s.append(np.full(deg, row, dtype=np.uint32))
+        extra_d.append(rng.choice(n, deg, replace=False).astype(np.uint32))
+    if heavy:
+        src = np.concatenate([src] + extra_s)
+        dst = np.concatenate([dst] + extra_d)
+    return src, dst
+
+
+def _dense(rng, shape, dt, integer=False):
+    if dt in (np.int32, np.int64) or integer:
+        return rng.integers(-8, 9, shape).astype(dt)
+    return rng.standard_normal(shape).astype(dt)
+
+
+def _to_torch(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def _gpu_spmm(torch, m, X, out_dtype=None, s_in=None, s_out=None):
+    x = _to_torch(torch, X)
+    y = torch.empty((m.get_num_rows(), X.shape[1]), dtype=out_dtype or x.dtype, device="cuda")
+    y.fill_(float("nan") if y.dtype.is_floating_point else -7)
+    si = _to_torch(torch, s_in) if s_in is not None else None
+    so = _to_torch(torch, s_out) if s_out is not None else None
+    assert m.multiply(x, y, si, so), _lib.last_error()
+    torch.cuda.synchronize()
+    return y.float().cpu().numpy() if y.dtype == torch.bfloat16 else y.cpu().numpy()
+
+
+CASES = [
+    # n, m, block, weighted dtype, dedup, heavy rows (row, degree)
+    (1000, 6000, (64, 128), None, False, ()),
+    (5000, 60000, (1024, 1024), np.float32, True, ()),
+    (20000, 100000, (16384, 16384), None, True, ((7, 20000), (11, 900), (13, 600))),
+    (20000, 100000, (4096, 2048), np.float32, False, ((3, 17000), (5, 5000))),
+    (3000, 20000, (256, 256), np.float64, True, ((1, 2999),)),
+]
+
+
+@pytest.mark.parametrize("case", range(len(CASES)))
+@pytest.mark.parametrize("k", [1, 2, 3, 4, 8, 10, 16, 32, 64, 130])
+def test_parity_float(torch_cuda, case, k):
+    torch = torch_cuda
+    n, mm, block, wdt, dedup, heavy = CASES[case]
+    src, dst = _graph(n, mm, 100 + case, heavy)
+    rng = np.random.default_rng(case * 1000 + k)
+    vals = None if wdt is None else rng.uniform(0.0, 1.0, len(src)).astype(wdt)
+    idx, mat = oracle.build_image(src, dst, vals, block=block, dedup=dedup)
+    img = matrix_image.from_bytes(idx, mat)
+    m = sparse_matrix.create(img, None, device=0)
+    dt = np.float64 if wdt is np.float64 else np.float32
+    has_split = any(d > 512 for _, d in heavy)
+    for integer in (True, False):
+        X = _dense(rng, (n, k), dt, integer)
+        Y = _gpu_spmm(torch, m, X)
+        R = oracle.spmm(idx, mat, X, nthreads=4)
+        if not has_split or (integer and wdt is None):
+            assert np.array_equal(Y.view(np.uint8), R.view(np.uint8)), (
+                f"not bit-exact: max diff {np.max(np.abs(Y - R))}")
+        else:
+            np.testing.assert_allclose(Y, R, rtol=RTOL, atol=RTOL * np.abs(R).max())
+
+
+@pytest.mark.parametrize("dt", [np.int32, np.int64])
+@pytest.mark.parametrize("k", [1, 4, 5, 16])
+def test_parity_integer(torch_cuda, dt, k):
+    torch = torch_cuda
+    src, dst = _graph(6000, 50000, 7, ((2, 20000),))
+    rng = np.random.default_rng(k)
+    vals = rng.integers(-3, 4, len(src)).astype(np.int32 if dt is np.int32 else np.int64)
+    for w in (None, vals):
+        idx, mat = oracle.build_image(src, dst, w, block=(2048, 2048), dedup=True)
+        m = sparse_matrix.create(matrix_image.from_bytes(idx, mat), None)
+        X = rng.integers(-1000, 1000, (6000, k)).astype(dt)
+        assert np.array_equal(_gpu_spmm(torch, m, X), oracle.spmm(idx, mat, X))
+
+
+def test_rand_mat_gen_known_answer(torch_cuda):
+    """matrix/test/rand_mat_gen.cpp:178-199: a binary matrix times
+    [0, 1, ..., ncol-1] equals each row's sum of column ids (duplicates kept)."""
+    torch = torch_cuda
+    rng = np.random.default_rng(11)
+    nrow, ncol = 30000, 20000
+    deg = rng.integers(0, 60, nrow)
+    src = np.repeat(np.arange(nrow, dtype=np.uint32), deg)
+    dst = rng.integers(0, ncol, len(src)).astype(np.uint32)
+    m = create_2d_matrix(src, dst, None, block_size=(4096, 4096), nrows=nrow, ncols=ncol)
+    X = np.arange(ncol, dtype=np.int64)[:, None]
+    Y = _gpu_spmm(torch, m, X)[:, 0]
+    keep = src != dst
+    expect = np.bincount(src[keep], weights=dst[keep].astype(np.float64), minlength=nrow).astype(np.int64)
+    assert np.array_equal(Y, expect)
+
+
+def test_bf16_input(torch_cuda):
+    torch = torch_cuda
+    src, dst = _graph(8000, 80000, 3)
+    idx, mat = oracle.build_image(src, dst, None, block=(4096, 4096), dedup=True)
+    m = sparse_matrix.create(matrix_image.from_bytes(idx, mat), None)
+    rng = np.random.default_rng(5)
+    for k in (8, 16, 32, 6):
+        Xf = rng.standard_normal((8000, k)).astype(np.float32)
+        xb = torch.from_numpy(Xf).to(torch.bfloat16).cuda()
+        Xr = xb.float().cpu().numpy()          # the bf16-rounded operand
+        y = torch.empty((8000, k), dtype=torch.float32, device="cuda")
+        assert m.multiply(xb, y)
+        R = oracle.spmm(idx, mat, Xr)
+        assert np.array_equal(y.cpu().numpy(), R)
+        yb = torch.empty((8000, k), dtype=torch.bfloat16, device="cuda")
+        assert m.multiply(xb, yb)
+        assert torch.equal(yb.cpu(), torch.from_numpy(R).to(torch.bfloat16))
+
+
+def test_row_scales(torch_cuda):
+    """y = D_out A D_in x, the normalised-adjacency operator of
+    matrix/test/test-eigen.cpp:88-136 (scale_rows, SpMM, scale_rows)."""
+    torch = torch_cuda
+    src, dst = _graph(10000, 90000, 9, ((4, 18000),))
+    idx, mat = oracle.build_image(src, dst, None, block=(8192, 8192), dedup=True)
+    m = sparse_matrix.create(matrix_image.from_bytes(idx, mat), None)
+    rng = np.random.default_rng(2)
+    for dt in (np.float32, np.float64):
+        X = rng.standard_normal((10000, 16)).astype(dt)
+        s_in = rng.uniform(0.1, 2.0, 10000).astype(dt)
+        s_out = rng.uniform(0.1, 2.0, 10000).astype(dt)
+        Y = _gpu_spmm(torch, m, X, s_in=s_in, s_out=s_out)
+        R = oracle.spmm(idx, mat, (X * s_in[:, None]).astype(dt)) * s_out[:, None]
+        np.testing.assert_allclose(Y, R, rtol=RTOL if dt == np.float32 else 1e-12,
+                                   atol=(RTOL if dt == np.float32 else 1e-12) * np.abs(R).max())
+
+
+def test_asymmetric_transpose(torch_cuda):
+    torch = torch_cuda
+    rng = np.random.default_rng(4)
+    src = rng.integers(0, 4000, 30000).astype(np.uint32)
+    dst = rng.integers(0, 4000, 30000).astype(np.uint32)
+    m, img, timg = create_2d_matrix(src, dst, None, block_size=(1024, 1024), is_sym=False, return_images=True)
+    assert not m.is_symmetric()
+    X = rng.integers(-8, 9, (m.get_num_cols(), 8)).astype(np.float32)
+    t = m.transpose()
+    i, a = img.bytes()
+    ti, ta = timg.bytes()
+    assert np.array_equal(_gpu_spmm(torch, m, X), oracle.spmm(i, a, X))
+    assert np.array_equal(_gpu_spmm(torch, t, X), oracle.spmm(ti, ta, X))
+
+
+def test_rmat_s18_parity(torch_cuda):
+    torch = torch_cuda
+    src, dst = rmat_edges(18, seed=1)
+    rng = np.random.default_rng(0)
+    for weighted in (False, True):
+        vals = rng.uniform(0.0, 1.0, len(src)).astype(np.float32) if weighted else None
+        vals = None if vals is None else np.where(vals == 0, np.float32(1.0), vals)
+        img = matrix_image.build(src, dst, vals, nrows=1 << 18, ncols=1 << 18, block_size=(16384, 16384),
+                                 dedup=True)
+        idx, mat = img.bytes()
+        m = sparse_matrix.create(img, None)
+        for k in (1, 4, 16, 32):
+            Xi = rng.integers(-8, 9, (1 << 18, k)).astype(np.float32)
+            assert np.array_equal(_gpu_spmm(torch, m, Xi), oracle.spmm(idx, mat, Xi, nthreads=8))
+            Xf = rng.standard_normal((1 << 18, k)).astype(np.float32)
+            R = oracle.spmm(idx, mat, Xf, nthreads=8)
+            np.testing.assert_allclose(_gpu_spmm(torch, m, Xf), R, rtol=RTOL, atol=RTOL * np.abs(R).max())
+
+
+def test_host_buffers_e2e(torch_cuda):
+    src, dst = _graph(5000, 40000, 21)
+    idx, mat = oracle.build_image(src, dst, None, block=(1024, 1024), dedup=True)
+    m = sparse_matrix.create(matrix_image.from_bytes(idx, mat), None)
+    X = np.random.default_rng(1).integers(-8, 9, (5000, 16)).astype(np.float32)
+    assert np.array_equal(m.multiply_host(X), oracle.spmm(idx, mat, X))
+
+
+def test_multiply_errors(torch_cuda):
+    """Dimension and type mismatches return False, like the reference."""
+    torch = torch_cuda
+    src, dst = _graph(1000, 5000, 1)
+    m = create_2d_matrix(src, dst, None, block_size=(256, 256), nrows=1000, ncols=1000)
+    x = torch.zeros((999, 4), device="cuda")
+    y = torch.zeros((1000, 4), device="cuda")
+    assert not m.multiply(x, y)
+    x = torch.zeros((1000, 4), device="cuda")
+    assert not m.multiply(x, torch.zeros((1000, 4), dtype=torch.float64, device="cuda"))
+    assert m.multiply(x, y)
