@@ -261,13 +261,18 @@ class sparse_matrix:
         if xt is None or yt is None:
             log.error("unsupported dense type %s -> %s", x.dtype, y.dtype)
             return False
-        if x.stride(1) != 1 or y.stride(1) != 1 or not x.is_cuda or not y.is_cuda:
+        def rowmajor(t):
+            return t.shape[1] == 1 or t.stride(1) == 1
+
+        if not (rowmajor(x) and rowmajor(y)) or not x.is_cuda or not y.is_cuda:
             log.error("dense matrices must be row-major CUDA tensors")
             return False
+        ldx = x.stride(0) if x.shape[0] > 1 else x.shape[1]
+        ldy = y.stride(0) if y.shape[0] > 1 else y.shape[1]
         sin = row_scale_in.data_ptr() if row_scale_in is not None else None
         sout = row_scale_out.data_ptr() if row_scale_out is not None else None
         st = stream if stream is not None else torch.cuda.current_stream(x.device).cuda_stream
-        rc = lib.fmx_spmm(self._h, xt, x.data_ptr(), x.stride(0), yt, y.data_ptr(), y.stride(0), x.shape[1],
+        rc = lib.fmx_spmm(self._h, xt, x.data_ptr(), ldx, yt, y.data_ptr(), ldy, x.shape[1],
                           sin, sout, st)
         if rc != _lib.FMX_OK:
             log.error("fmx_spmm: %s", _lib.last_error())
