@@ -245,6 +245,7 @@ def main():
     create_s = time.time() - t0
     n_rows, n_cols, nnz, k = inf["nrows"], inf["ncols"], inf["nnz"], a.k
     light, tasks, heavy, kernels = m.schedule()
+    n_hot, hot_entries, scratch_bytes = m.hot()
     cpu_img = img if (rank == 0 and world == 1 and not a.skip_cpu) else None
     if cpu_img is None:
         del img
@@ -342,10 +343,12 @@ def main():
                              % (n_cols * k * 4 / 1e9, nnz * 4 / 1e9),
                        "parallelism": f"replicas{world}" if world > 1 else "single",
                        "host_build_s": round(build_s, 2), "device_create_s": round(create_s, 2),
-                       "schedule": {"light_rows": light, "warp_tasks": tasks, "heavy_rows": heavy}},
+                       "schedule": {"exact_rows": light, "ranges": tasks, "long_rows": heavy,
+                                    "hot_cols": n_hot, "hot_entry_frac": round(hot_entries / max(nnz, 1), 4),
+                                    "scratch_bytes": scratch_bytes}},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
-                         "kernel": "spmm_kernel (+ spmm_fixup_kernel), per fmx_spmm call",
+                         "kernel": "pack_hot_kernel + spmm_kernel + spmm_fixup_kernel, per fmx_spmm call",
                          "traffic": traffic},
             "cpu_baseline": cpu,
             "e2e": e2e,

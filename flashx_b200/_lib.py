@@ -22,6 +22,8 @@ FMX_ERR_UNSUPPORTED = -8
 F32, F64, BF16, I32, I64 = 0, 1, 2, 3, 4
 P_BOOL, P_INTEGER, P_LONG, P_FLOAT, P_DOUBLE = 0, 4, 6, 8, 9
 
+EXACT_ROW_MAX = 256   # FMX_EXACT_ROW_MAX: rows summed in the reference's order
+
 BUILD_DEDUP = 0x1
 BUILD_KEEP_SELF_LOOPS = 0x2
 BUILD_REF_VALUE_LAYOUT = 0x4
@@ -67,6 +69,7 @@ _SIGS = {
     "fmx_spmm": (_int, [_vp, _int, _vp, _i64, _int, _vp, _i64, _i64, _vp, _vp, _vp]),
     "fmx_spmm_host": (_int, [_vp, _int, _vp, _i64, _int, _vp, _i64, _i64]),
     "fmx_matrix_schedule": (_int, [_vp, _P(_u64), _P(_u64), _P(_u64), _P(_u64)]),
+    "fmx_matrix_hot": (_int, [_vp, _P(_u64), _P(_u64), _P(_u64)]),
     "fmx_rmat_edges_host": (_int, [_int, _u64, _d, _d, _d, _u64, _int, _vp, _vp, _int]),
     "fmx_rmat_edges_device": (_int, [_int, _u64, _d, _d, _d, _u64, _int, _vp, _vp, _vp]),
 }

@@ -4,25 +4,53 @@
 // block_spmm_task_impl::run_on_block, matrix/sparse_matrix.h:219-375, driven
 // by block_compute_task::run, matrix/sparse_matrix.cpp:251-314).
 //
-// Layout in HBM (built once per matrix, kept resident):
-//   row_ptr  uint32[nrows+1]   rows of the decoded 2D image, ascending
-//   col      int32 [nnz]       global column ids, per row in the order the
-//                              reference visits them (ascending block column,
-//                              then ascending column)
-//   val      entry[nnz]        only for weighted images
-//   light    int32 [n_light]   rows of degree <= kLightMax, degree-sorted
-//                              (descending) inside bands of kBand rows
-//   tasks    split_task[]      rows longer than kLightMax: one warp per row
-//                              (medium) or per kChunk-entry chunk (heavy)
-//   heavy    heavy_row[]       heavy rows: their chunks' partial sums are added
-//                              in chunk order by spmm_fixup_kernel
-//   partial  AccT[n_partials][kPartialStride] scratch for heavy chunks
+// Layout in HBM (built once per matrix from the decoded 2D image, resident):
+//   col      uint32[]           one entry stream.  Bit 31 is set on the last
+//                               entry of a row; with bit 30 set, bits 0-29 hold
+//                               a hot slot, else the column id.  First every
+//                               row in ascending order: a row of 1..kExactMax
+//                               entries as its entries in the order the
+//                               reference visits them (ascending block column,
+//                               then column); an empty or longer row as one
+//                               entry naming the pack's zero row.  Then the
+//                               entries of the longer rows (> kExactMax).
+//   val      entry[]            only for weighted images, same order
+//   hot_col  int32[H]           the H <= kHotMax columns of highest in-degree;
+//                               entry slot s + 1 names hot_col[s], slot 0 the
+//                               pack's zero row
+//   ranges   range_t[]          work units, sorted by entry count (largest
+//                               first): a run of consecutive rows of ~kRange
+//                               entries, or one of the equal chunks (<= kChunk
+//                               entries) of a longer row.  Each starts at a
+//                               multiple of 8 entries and is padded to one
+//                               with zero-row entries (after the last row end
+//                               of a run they are never stored; in a chunk
+//                               they add zeros), so steps need no bounds.
+//   heavy    heavy_row[]        longer rows: spmm_fixup_kernel overwrites their
+//                               Y rows with their chunk partials added in
+//                               chunk order
+// Scratch (allocated with the matrix):
+//   xhot     (H+1) x 128 bytes  per call, the hot columns' X rows of the
+//                               current panel, packed back to back (times s_in
+//                               when given) after row 0, which stays zero
+//   partial  AccT[chunks][kPartialStride]  chunk sums of longer rows
 //
-// Work units: a warp is split into R = floor(32/G) lane groups of G lanes;
-// a group owns one output row of a light warp and sums its entries
-// sequentially in ascending column order (the reference's order), loading
-// each X row as G 16-byte vectors.  No atomics: every output row is written
-// by exactly one group (light), one warp (medium) or the fixup warp (heavy).
+// Why the hot pack: the X gathers of an R-MAT graph are random 64-byte reads
+// that mostly miss the L2, and a hot row shares its 128-byte line with a cold
+// one.  Packing the highest in-degree rows (about 87% of the gathers at scale
+// 24) two to a line, read with an L2 evict_last hint while the cold rows and
+// the streams use evict_first, keeps them resident.
+//
+// Execution: a persistent grid.  A warp is split into R = floor(32/G) lane
+// groups of G lanes; a lane loads 16 bytes of an X row, so G lanes cover a
+// row of k elements.  Lane groups take ranges round-robin and walk them as a
+// stream of entries in aligned steps of U (4 or 8): a step loads its column
+// ids with 16-byte loads, issues its U gathers together with the next step's
+// column-id loads, then adds them up in entry order; when an entry closes a
+// row the group stores that row (the range's first row plus the rows closed
+// before it).  Every row of up to kExactMax
+// entries is summed by one group in the reference's order (bit-identical
+// results).  No atomics: every output row is written exactly once.
 #include "fmx_internal.h"
 
 #include <cuda_runtime.h>
@@ -30,6 +58,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <mutex>
 #include <thread>
 
@@ -38,17 +67,27 @@ namespace fmx {
 // ---------------------------------------------------------------------------
 // Schedule parameters
 // ---------------------------------------------------------------------------
-constexpr uint32_t kLightMax = 512;     // rows summed by one lane group
-constexpr uint32_t kHeavyMin = 16384;   // rows split into chunks above this
-constexpr uint32_t kChunk = 4096;       // entries per heavy chunk
-constexpr uint32_t kBand = 65536;       // degree sort stays inside row bands
+constexpr uint32_t kExactMax = FMX_EXACT_ROW_MAX;  // rows summed by one lane group
+constexpr uint32_t kChunk = 256;        // most entries per chunk of a longer row
+constexpr uint32_t kRange = 256;        // target entries per multi-row range
+constexpr uint32_t kHotMax = 1u << 20;  // most packed hot columns
+constexpr int kPanelBytes = 128;        // X row bytes per panel (hot pack row)
 constexpr int kPartialStride = 256;     // AccT slots per partial (one panel)
 constexpr int kThreads = 256;           // threads per SpMM block
+#ifndef FMX_SPMM_MIN_BLOCKS
+#define FMX_SPMM_MIN_BLOCKS 5           // resident blocks per SM the register budget targets
+#endif
+constexpr int kStep = 8;                // entries per index load group (alignment unit)
+constexpr uint32_t kEnd = 0x80000000u;  // last entry of a row
+constexpr uint32_t kHot = 0x40000000u;  // entry refers to a hot slot
+constexpr uint32_t kIdxMask = 0x3FFFFFFFu;
+constexpr uint32_t kNoSlot = 0xFFFFFFFFu;
 
-struct split_task {
-	int32_t row;
-	uint32_t start, end;
-	int32_t slot;        // -1: write Y[row]; else partial slot
+struct range_t {
+	uint32_t e0;         // first entry (a multiple of kStep)
+	uint32_t len;        // entries, padded to a multiple of kStep
+	uint32_t row0;       // first row (row runs)
+	uint32_t slot;       // kNoSlot for row runs; else the chunk's partial slot
 };
 struct heavy_row {
 	int32_t row;
@@ -69,17 +108,19 @@ struct gpu_part {
 	uint64_t nrows = 0, ncols = 0, nnz = 0;
 	int prim = 0;
 	size_t esize = 0;
-	uint32_t *row_ptr = nullptr;
-	int32_t *col = nullptr;
+	uint32_t *col = nullptr;
 	void *val = nullptr;
-	int32_t *light = nullptr;
-	uint32_t n_light = 0;
-	split_task *tasks = nullptr;
-	uint32_t n_tasks = 0;
+	int32_t *hot_col = nullptr;
+	uint32_t n_hot = 0;
+	void *xhot = nullptr;                // (n_hot + 1) * kPanelBytes
+	uint32_t n_exact = 0;                // rows summed in the reference's order
+	range_t *ranges = nullptr;
+	uint32_t n_ranges = 0;
 	heavy_row *heavy = nullptr;
 	uint32_t n_heavy = 0;
 	uint32_t n_partials = 0;
 	void *partial = nullptr;
+	uint64_t hot_entries = 0;            // entries that read the hot pack
 	uint64_t bytes = 0;
 	// staging buffers of fmx_spmm_host (grow-only, guarded by stage_mu)
 	std::mutex stage_mu;
@@ -89,7 +130,7 @@ struct gpu_part {
 		int cur = 0;
 		cudaGetDevice(&cur);
 		cudaSetDevice(device);
-		void *ps[] = {row_ptr, col, val, light, tasks, heavy, partial, stage_x, stage_y};
+		void *ps[] = {col, val, hot_col, xhot, ranges, heavy, partial, stage_x, stage_y};
 		for (void *p : ps)
 			if (p) cudaFree(p);
 		cudaSetDevice(cur);
@@ -130,14 +171,33 @@ template <class A> __device__ __forceinline__ A to_acc(__nv_bfloat16 v) { return
 template <class Y, class A> __device__ __forceinline__ Y from_acc(A v) { return Y(v); }
 template <> __device__ __forceinline__ __nv_bfloat16 from_acc<__nv_bfloat16, float>(float v) { return __float2bfloat16_rn(v); }
 
-// Streaming loads/stores for the index stream and the output (touched once,
-// evict-first in L1 and L2) so that the gathered X rows keep the L2.
-__device__ __forceinline__ int32_t ld_stream(const int32_t *p) { return __ldcs(p); }
+// Packed FP32 pairs (sm_100 add.rn.f32x2): two IEEE round-to-nearest adds
+// per instruction, the same results as two scalar adds.
+__device__ __forceinline__ uint64_t pack2(float a, float b)
+{
+	uint64_t r;
+	asm("mov.b64 %0, {%1,%2};" : "=l"(r) : "f"(a), "f"(b));
+	return r;
+}
+__device__ __forceinline__ void unpack2(uint64_t v, float &a, float &b)
+{
+	asm("mov.b64 {%0,%1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+}
+__device__ __forceinline__ uint64_t add2(uint64_t a, uint64_t b)
+{
+	uint64_t r;
+	asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+	return r;
+}
+
+// Streaming (read-once) loads and stores: evict-first in L1 and L2 so that
+// the gathered X rows keep the caches.
 __device__ __forceinline__ float ld_stream(const float *p) { return __ldcs(p); }
 __device__ __forceinline__ double ld_stream(const double *p) { return __ldcs(p); }
+__device__ __forceinline__ int32_t ld_stream(const int32_t *p) { return __ldcs(p); }
 __device__ __forceinline__ int64_t ld_stream(const int64_t *p) { return (int64_t)__ldcs((const long long *)p); }
 
-// A 16-byte vector of VEC elements of T (VEC * sizeof(T) == 16), or a scalar.
+// VEC elements of T: one 16-byte vector, or a scalar (VEC == 1).
 template <class T, int VEC>
 struct xvec {
 	T v[VEC];
@@ -150,18 +210,13 @@ __device__ __forceinline__ xvec<T, VEC> ld_x(const T *p)
 	if constexpr (VEC * sizeof(T) == 16) {
 		uint4 u = __ldg(reinterpret_cast<const uint4 *>(p));
 		memcpy(&r, &u, 16);
+	} else if constexpr (sizeof(T) == 2) {
+		unsigned short u = __ldg(reinterpret_cast<const unsigned short *>(p));
+		memcpy(&r, &u, 2);
 	} else {
 		static_assert(VEC == 1, "scalar path");
 		r.v[0] = __ldg(p);
 	}
-	return r;
-}
-template <>
-__device__ __forceinline__ xvec<__nv_bfloat16, 1> ld_x<__nv_bfloat16, 1>(const __nv_bfloat16 *p)
-{
-	xvec<__nv_bfloat16, 1> r;
-	unsigned short u = __ldg(reinterpret_cast<const unsigned short *>(p));
-	memcpy(&r.v[0], &u, 2);
 	return r;
 }
 
@@ -187,104 +242,141 @@ __device__ __forceinline__ void st_y(T *p, const T (&v)[VEC])
 	}
 }
 
+// L2 eviction priorities for the gathers (createpolicy, PTX ISA 7.4+).
+__device__ __forceinline__ uint64_t policy_evict_last()
+{
+	uint64_t p;
+	asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+	return p;
+}
+__device__ __forceinline__ uint64_t policy_evict_first()
+{
+	uint64_t p;
+	asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+	return p;
+}
+
+// Read-only gather of VEC elements of T (16 bytes, or one scalar) with an L2
+// eviction-priority hint.
+template <class T, int VEC>
+__device__ __forceinline__ xvec<T, VEC> ld_x_hint(const T *p, uint64_t pol)
+{
+	xvec<T, VEC> r;
+	if constexpr (VEC * sizeof(T) == 16) {
+		uint32_t a, b, c, d;
+		asm volatile("ld.global.nc.L2::cache_hint.v4.u32 {%0,%1,%2,%3}, [%4], %5;"
+				: "=r"(a), "=r"(b), "=r"(c), "=r"(d) : "l"(p), "l"(pol));
+		uint4 u = make_uint4(a, b, c, d);
+		memcpy(&r, &u, 16);
+	} else if constexpr (sizeof(T) == 8) {
+		static_assert(VEC == 1, "scalar path");
+		uint64_t a;
+		asm volatile("ld.global.nc.L2::cache_hint.u64 %0, [%1], %2;" : "=l"(a) : "l"(p), "l"(pol));
+		memcpy(&r, &a, 8);
+	} else if constexpr (sizeof(T) == 4) {
+		static_assert(VEC == 1, "scalar path");
+		uint32_t a;
+		asm volatile("ld.global.nc.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(a) : "l"(p), "l"(pol));
+		memcpy(&r, &a, 4);
+	} else {
+		static_assert(VEC == 1 && sizeof(T) == 2, "scalar path");
+		unsigned short a;
+		asm volatile("ld.global.nc.L2::cache_hint.u16 %0, [%1], %2;" : "=h"(a) : "l"(p), "l"(pol));
+		memcpy(&r, &a, 2);
+	}
+	return r;
+}
+
 struct spmm_args {
-	const uint32_t *row_ptr;
-	const int32_t *col;
+	const uint32_t *col;
 	const void *val;
-	const int32_t *light;
-	const split_task *tasks;
+	const range_t *ranges;
 	const void *X;
+	const void *xhot;    // packed hot rows of this panel, row stride hot_ld
 	void *Y;
 	const void *s_in;
 	const void *s_out;
 	void *partial;
 	int64_t ldx, ldy;
+	int hot_ld;      // elements per packed hot row
 	int k;           // columns in this panel
 	int G;           // lanes per row group
 	int R;           // row groups per warp
-	int nv;          // vectors per lane (generic path)
-	uint32_t n_light;
-	uint32_t n_tasks;
-	uint64_t n_light_warps;
+	int nv;          // vectors per lane (scalar path)
+	uint32_t n_ranges;
 };
 
-// WT = void for a binary matrix (every entry is 1).
-template <class WT, class A>
-__device__ __forceinline__ A ld_w(const void *val, uint32_t e)
-{
-	if constexpr (std::is_void<WT>::value) {
-		return A(1);
-	} else {
-		return A(ld_stream(static_cast<const WT *>(val) + e));
-	}
-}
+// The running sums of one lane: NV vectors of VEC elements.  FP32 with
+// VEC == 4 or 8 is kept as packed pairs.
+template <class A, int VEC, int NV>
+struct accum {
+	static constexpr bool kPacked = std::is_same<A, float>::value && (VEC % 2 == 0) && NV == 1;
+	A s[NV][VEC];
+	uint64_t p[VEC / 2 > 0 ? VEC / 2 : 1];
 
-// Sum entries [e0, e1) of one row into acc (NV vectors of VEC per lane).
-// Lane columns: c0 + v * G * VEC + [0, VEC).
-template <class XT, class A, class WT, int VEC, int NV, bool SCALE_IN>
-__device__ __forceinline__ void row_sum(const spmm_args &a, uint32_t e0, uint32_t e1,
-		int colbase, int nv, A (&acc)[NV][VEC])
-{
-	const XT *X = static_cast<const XT *>(a.X);
-	const A *sin = static_cast<const A *>(a.s_in);
-	const int stride = a.G * VEC;
-	constexpr int U = (NV == 1) ? 8 : 2;
-	uint32_t e = e0;
-	for (; e + U <= e1; e += U) {
-		int32_t c[U];
+	__device__ __forceinline__ void zero()
+	{
+		if constexpr (kPacked) {
 #pragma unroll
-		for (int u = 0; u < U; u++) c[u] = ld_stream(a.col + e + u);
-		A w[U], sc[U];
+			for (int i = 0; i < VEC / 2; i++) p[i] = 0;
+		} else {
 #pragma unroll
-		for (int u = 0; u < U; u++) w[u] = ld_w<WT, A>(a.val, e + u);
-		if constexpr (SCALE_IN) {
+			for (int v = 0; v < NV; v++)
 #pragma unroll
-			for (int u = 0; u < U; u++) sc[u] = sin[c[u]];
+				for (int i = 0; i < VEC; i++) s[v][i] = A(0);
 		}
-		xvec<XT, VEC> x[U][NV];
-#pragma unroll
-		for (int u = 0; u < U; u++)
-#pragma unroll
-			for (int v = 0; v < NV; v++)
-				if (v < nv && colbase + v * stride < a.k)
-					x[u][v] = ld_x<XT, VEC>(X + int64_t(c[u]) * a.ldx + colbase + v * stride);
-#pragma unroll
-		for (int u = 0; u < U; u++)
-#pragma unroll
-			for (int v = 0; v < NV; v++)
-				if (v < nv && colbase + v * stride < a.k)
-#pragma unroll
-					for (int i = 0; i < VEC; i++) {
-						// (x * s_in) * w, rounded per step like scale_rows then SpMM
-						A xv = to_acc<A>(x[u][v].v[i]);
-						if constexpr (SCALE_IN) xv = acc_mul(xv, sc[u]);
-						if constexpr (!std::is_void<WT>::value) xv = acc_mul(xv, w[u]);
-						acc[v][i] = acc_add(acc[v][i], xv);
-					}
 	}
-	for (; e < e1; e++) {
-		int32_t c = ld_stream(a.col + e);
-		A w = ld_w<WT, A>(a.val, e);
-		A sc = A(1);
-		if constexpr (SCALE_IN) sc = sin[c];
+	__device__ __forceinline__ void zero_if(bool z)
+	{
+		if constexpr (kPacked) {
 #pragma unroll
-		for (int v = 0; v < NV; v++)
-			if (v < nv && colbase + v * stride < a.k) {
-				xvec<XT, VEC> x = ld_x<XT, VEC>(X + int64_t(c) * a.ldx + colbase + v * stride);
+			for (int i = 0; i < VEC / 2; i++) p[i] = z ? 0ull : p[i];
+		} else {
 #pragma unroll
-				for (int i = 0; i < VEC; i++) {
-					A xv = to_acc<A>(x.v[i]);
-					if constexpr (SCALE_IN) xv = acc_mul(xv, sc);
-					if constexpr (!std::is_void<WT>::value) xv = acc_mul(xv, w);
-					acc[v][i] = acc_add(acc[v][i], xv);
-				}
+			for (int v = 0; v < NV; v++)
+#pragma unroll
+				for (int i = 0; i < VEC; i++) s[v][i] = z ? A(0) : s[v][i];
+		}
+	}
+	// s[v] += x (* m1) (* m2), each operation rounded (no contraction)
+	template <class XT, int NMUL>
+	__device__ __forceinline__ void add(int v, const xvec<XT, VEC> &x, A m1, A m2)
+	{
+		if constexpr (kPacked) {
+			// products stay scalar __fmul_rn (never fused into the add);
+			// only the adds are packed
+#pragma unroll
+			for (int i = 0; i < VEC / 2; i++) {
+				float t0 = to_acc<float>(x.v[2 * i]), t1 = to_acc<float>(x.v[2 * i + 1]);
+				if constexpr (NMUL >= 1) { t0 = __fmul_rn(t0, m1); t1 = __fmul_rn(t1, m1); }
+				if constexpr (NMUL >= 2) { t0 = __fmul_rn(t0, m2); t1 = __fmul_rn(t1, m2); }
+				p[i] = add2(p[i], pack2(t0, t1));
 			}
+		} else {
+#pragma unroll
+			for (int i = 0; i < VEC; i++) {
+				A t = to_acc<A>(x.v[i]);
+				if constexpr (NMUL >= 1) t = acc_mul(t, m1);
+				if constexpr (NMUL >= 2) t = acc_mul(t, m2);
+				s[v][i] = acc_add(s[v][i], t);
+			}
+		}
 	}
-}
+	__device__ __forceinline__ A get(int v, int i) const
+	{
+		if constexpr (kPacked) {
+			float a, b;
+			unpack2(p[i / 2], a, b);
+			return (i & 1) ? b : a;
+		} else {
+			return s[v][i];
+		}
+	}
+};
 
 template <class YT, class A, int VEC, int NV, bool SCALE_OUT>
-__device__ __forceinline__ void store_row(const spmm_args &a, int32_t row, int colbase, int nv,
-		const A (&acc)[NV][VEC])
+__device__ __forceinline__ void store_row(const spmm_args &a, int32_t row, int colbase,
+		const accum<A, VEC, NV> &acc)
 {
 	YT *Y = static_cast<YT *>(a.Y);
 	A so = A(1);
@@ -292,11 +384,11 @@ __device__ __forceinline__ void store_row(const spmm_args &a, int32_t row, int c
 	const int stride = a.G * VEC;
 #pragma unroll
 	for (int v = 0; v < NV; v++)
-		if (v < nv && colbase + v * stride < a.k) {
+		if (v < a.nv && colbase + v * stride < a.k) {
 			YT out[VEC];
 #pragma unroll
 			for (int i = 0; i < VEC; i++) {
-				A t = acc[v][i];
+				A t = acc.get(v, i);
 				if constexpr (SCALE_OUT) t = acc_mul(t, so);
 				out[i] = from_acc<YT, A>(t);
 			}
@@ -304,69 +396,147 @@ __device__ __forceinline__ void store_row(const spmm_args &a, int32_t row, int c
 		}
 }
 
-template <class XT, class YT, class A, class WT, int VEC, int NV, bool SCALE_IN, bool SCALE_OUT>
-__global__ void __launch_bounds__(kThreads)
-spmm_kernel(const spmm_args a)
+template <int U>
+__device__ __forceinline__ void ld_idx(const uint32_t *col, uint32_t step, uint32_t (&r)[U])
 {
-	__shared__ A red[kThreads / 32][32][NV * VEC];
-	const int lane = threadIdx.x & 31;
-	const int wib = threadIdx.x >> 5;
-	const uint64_t gw = (uint64_t(blockIdx.x) * kThreads + threadIdx.x) >> 5;
-	const int G = a.G, R = a.R;
-	const int grp = lane / G;
-	const int sub = lane - grp * G;
-	const int colbase = sub * VEC;
-	A acc[NV][VEC];
+	const uint4 *p = reinterpret_cast<const uint4 *>(col) + (U / 4) * step;
 #pragma unroll
-	for (int v = 0; v < NV; v++)
-#pragma unroll
-		for (int i = 0; i < VEC; i++) acc[v][i] = A(0);
+	for (int q = 0; q < U / 4; q++) {
+		// cached: a group reads each 128-byte line of its stream over several steps
+		uint4 a = __ldg(p + q);
+		r[4 * q] = a.x; r[4 * q + 1] = a.y; r[4 * q + 2] = a.z; r[4 * q + 3] = a.w;
+	}
+}
 
-	if (gw < a.n_tasks) {
-		// One long row (or one chunk of a heavy row) over all R groups: group g
-		// sums a contiguous 1/R of the entries; the group sums are then added
-		// in group order.
-		const split_task t = a.tasks[gw];
-		const uint32_t len = t.end - t.start;
-		if (grp < R) {
-			uint32_t b = t.start + uint32_t((uint64_t(len) * grp) / R);
-			uint32_t e = t.start + uint32_t((uint64_t(len) * (grp + 1)) / R);
-			row_sum<XT, A, WT, VEC, NV, SCALE_IN>(a, b, e, colbase, a.nv, acc);
+template <class WT, class A, int U>
+__device__ __forceinline__ void ld_w(const void *val, uint32_t step, A (&w)[U])
+{
+	if constexpr (std::is_void<WT>::value) {
+#pragma unroll
+		for (int u = 0; u < U; u++) w[u] = A(1);
+	} else {
+		const uint4 *p = reinterpret_cast<const uint4 *>(static_cast<const WT *>(val) + size_t(step) * U);
+		constexpr int per = int(16 / sizeof(WT));
+#pragma unroll
+		for (int q = 0; q < U / per; q++) {
+			uint4 a = __ldcs(p + q);
+			WT t[per];
+			memcpy(t, &a, 16);
+#pragma unroll
+			for (int i = 0; i < per; i++) w[q * per + i] = A(t[i]);
 		}
+	}
+}
+
+// One range in steps of U entries.  Row runs (slot == kNoSlot) store each
+// row when its end flag passes; chunks of longer rows leave their sum in
+// partial[slot].  Hot entries read the packed rows (which already carry
+// s_in); the others read X and, with SCALE_IN, s_in.
+template <class XT, class YT, class A, class WT, int VEC, int NV, int U, bool SCALE_IN, bool SCALE_OUT>
+__device__ __forceinline__ void run_range(const spmm_args &a, const range_t rg, int colbase,
+		uint64_t pol_hot, uint64_t pol_cold)
+{
+	const XT *X = static_cast<const XT *>(a.X);
+	const XT *H = static_cast<const XT *>(a.xhot);
+	const int stride = a.G * VEC;
+	constexpr bool kBinary = std::is_void<WT>::value;
+	const bool runs = rg.slot == kNoSlot;
+	accum<A, VEC, NV> acc;
+	acc.zero();
+	uint32_t row = rg.row0;
+	uint32_t s = rg.e0 / U;
+	const uint32_t s_end = s + rg.len / U;
+	uint32_t raw[U];
+	ld_idx<U>(a.col, s, raw);
+	for (; s < s_end; s++) {
+		A w[U];
+		if constexpr (!kBinary) ld_w<WT, A, U>(a.val, s, w);
+		// issue this step's gathers
+		xvec<XT, VEC> x[U][NV];
+		A sc[U];
+		uint32_t ends = 0;
+#pragma unroll
+		for (int u = 0; u < U; u++) {
+			const uint32_t c = raw[u] & kIdxMask;
+			const bool hot = raw[u] & kHot;
+			const XT *xr = (hot ? H : X) + int64_t(c) * (hot ? int64_t(a.hot_ld) : a.ldx) + colbase;
+			const uint64_t pol = hot ? pol_hot : pol_cold;
+#pragma unroll
+			for (int v = 0; v < NV; v++)
+				if (v < a.nv && colbase + v * stride < a.k)
+					x[u][v] = ld_x_hint<XT, VEC>(xr + v * stride, pol);
+			if constexpr (SCALE_IN) sc[u] = hot ? A(1) : static_cast<const A *>(a.s_in)[c];
+			ends |= (raw[u] >> 31) << u;
+		}
+		// the next step's column ids load while the gathers are in flight
+		if (s + 1 < s_end) ld_idx<U>(a.col, s + 1, raw);
+		// add up in entry order; a set end flag closes the row
+#pragma unroll
+		for (int u = 0; u < U; u++) {
+#pragma unroll
+			for (int v = 0; v < NV; v++)
+				if (v < a.nv && colbase + v * stride < a.k) {
+					// (x * s_in) * w, rounded per step like scale_rows then SpMM;
+					// for hot entries x * s_in was rounded by the pack
+					if constexpr (SCALE_IN && !kBinary) acc.template add<XT, 2>(v, x[u][v], sc[u], w[u]);
+					else if constexpr (SCALE_IN) acc.template add<XT, 1>(v, x[u][v], sc[u], A(1));
+					else if constexpr (!kBinary) acc.template add<XT, 1>(v, x[u][v], w[u], A(1));
+					else acc.template add<XT, 0>(v, x[u][v], A(1), A(1));
+				}
+			const bool end = runs && ((ends >> u) & 1u);
+			if (end) store_row<YT, A, VEC, NV, SCALE_OUT>(a, int32_t(row), colbase, acc);
+			acc.zero_if(end);
+			row += end;
+		}
+	}
+	if (!runs) {
+		A *p = static_cast<A *>(a.partial) + int64_t(rg.slot) * kPartialStride;
 #pragma unroll
 		for (int v = 0; v < NV; v++)
+			if (v < a.nv && colbase + v * stride < a.k)
 #pragma unroll
-			for (int i = 0; i < VEC; i++) red[wib][lane][v * VEC + i] = acc[v][i];
-		__syncwarp();
-		if (grp == 0) {
-			for (int g = 1; g < R; g++)
-#pragma unroll
-				for (int v = 0; v < NV; v++)
-#pragma unroll
-					for (int i = 0; i < VEC; i++)
-						acc[v][i] = acc_add(acc[v][i], red[wib][g * G + sub][v * VEC + i]);
-			if (t.slot < 0) {
-				store_row<YT, A, VEC, NV, SCALE_OUT>(a, t.row, colbase, a.nv, acc);
-			} else {
-				A *p = static_cast<A *>(a.partial) + int64_t(t.slot) * kPartialStride;
-				const int stride = G * VEC;
-#pragma unroll
-				for (int v = 0; v < NV; v++)
-					if (v < a.nv && colbase + v * stride < a.k)
-#pragma unroll
-						for (int i = 0; i < VEC; i++) p[colbase + v * stride + i] = acc[v][i];
-			}
-		}
-		return;
+				for (int i = 0; i < VEC; i++) p[colbase + v * stride + i] = acc.get(v, i);
 	}
-	const uint64_t lw = gw - a.n_tasks;
-	if (lw >= a.n_light_warps || grp >= R) return;
-	const uint64_t li = lw * R + grp;
-	if (li >= a.n_light) return;
-	const int32_t row = a.light[li];
-	const uint32_t e0 = a.row_ptr[row], e1 = a.row_ptr[row + 1];
-	row_sum<XT, A, WT, VEC, NV, SCALE_IN>(a, e0, e1, colbase, a.nv, acc);
-	store_row<YT, A, VEC, NV, SCALE_OUT>(a, row, colbase, a.nv, acc);
+}
+
+template <class XT, class YT, class A, class WT, int VEC, int NV, int U, bool SCALE_IN, bool SCALE_OUT>
+__global__ void __launch_bounds__(kThreads, FMX_SPMM_MIN_BLOCKS)
+spmm_kernel(const spmm_args a)
+{
+	const int lane = threadIdx.x & 31;
+	const uint32_t gw = (blockIdx.x * kThreads + threadIdx.x) >> 5;
+	const uint32_t nw = (gridDim.x * kThreads) >> 5;
+	const int G = a.G, R = a.R;
+	const int grp = lane / G;
+	if (grp >= R) return;
+	const int colbase = (lane - grp * G) * VEC;
+	const uint32_t gg = gw * uint32_t(R) + uint32_t(grp);
+	const uint32_t ng = nw * uint32_t(R);
+	const uint64_t pol_hot = policy_evict_last(), pol_cold = policy_evict_first();
+	for (uint32_t r = gg; r < a.n_ranges; r += ng)
+		run_range<XT, YT, A, WT, VEC, NV, U, SCALE_IN, SCALE_OUT>(a, a.ranges[r], colbase, pol_hot, pol_cold);
+}
+
+// Pack the hot columns' X rows of this panel behind a zero row:
+// xhot[0][j] = 0 and xhot[s+1][j] = X[hot_col[s]][c0 + j] (times
+// s_in[hot_col[s]], rounded, when SCALE_IN), j < kp.  The zero row is
+// rewritten every call because a narrower earlier panel packs over it.
+template <class XT, class A, bool SCALE_IN>
+__global__ void pack_hot_kernel(const int32_t *hot_col, uint32_t n_hot, const XT *X, int64_t ldx, int kp,
+		XT *xhot, int hot_ld, const A *s_in)
+{
+	const uint64_t total = uint64_t(n_hot + 1) * kp;
+	for (uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < total; t += uint64_t(gridDim.x) * blockDim.x) {
+		const uint32_t s = uint32_t(t / kp);
+		const int j = int(t - uint64_t(s) * kp);
+		XT v = XT(0);
+		if (s > 0) {
+			const int32_t c = __ldg(hot_col + s - 1);
+			v = X[int64_t(c) * ldx + j];
+			if constexpr (SCALE_IN) v = from_acc<XT, A>(acc_mul(to_acc<A>(v), s_in[c]));
+		}
+		xhot[int64_t(s) * hot_ld + j] = v;
+	}
 }
 
 // Heavy rows: add the chunk partials in chunk order, scale, convert, store.
@@ -392,96 +562,196 @@ __global__ void spmm_fixup_kernel(const heavy_row *heavy, uint32_t n_heavy, cons
 // ---------------------------------------------------------------------------
 
 template <class T>
-static int upload(T **dst, const T *src, size_t n, uint64_t &bytes)
+static int upload(T **dst, const T *src, size_t n, uint64_t &bytes, size_t alloc_n = 0)
 {
 	*dst = nullptr;
-	if (!n) return FMX_OK;
-	cudaError_t e = cudaMalloc(reinterpret_cast<void **>(dst), n * sizeof(T));
+	alloc_n = std::max(alloc_n, n);
+	if (!alloc_n) return FMX_OK;
+	cudaError_t e = cudaMalloc(reinterpret_cast<void **>(dst), alloc_n * sizeof(T));
 	if (e != cudaSuccess)
 		return set_error(e == cudaErrorMemoryAllocation ? FMX_ERR_OOM : FMX_ERR_CUDA,
-				"cudaMalloc of %zu bytes failed: %s", n * sizeof(T), cudaGetErrorString(e));
-	bytes += n * sizeof(T);
-	CUDA_TRY(cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice));
+				"cudaMalloc of %zu bytes failed: %s", alloc_n * sizeof(T), cudaGetErrorString(e));
+	bytes += alloc_n * sizeof(T);
+	if (n) CUDA_TRY(cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice));
+	if (alloc_n > n) CUDA_TRY(cudaMemset(reinterpret_cast<char *>(*dst) + n * sizeof(T), 0, (alloc_n - n) * sizeof(T)));
 	return FMX_OK;
+}
+
+template <class F>
+static void par_for(uint64_t n, F fn)
+{
+	int nt = std::max(1, std::min<int>(default_threads(), int((n + 65535) / 65536)));
+	std::vector<std::thread> th;
+	uint64_t per = (n + nt - 1) / nt;
+	for (int t = 0; t < nt; t++)
+		th.emplace_back([&, t]() {
+			uint64_t b = uint64_t(t) * per, e = std::min(n, b + per);
+			if (b < e) fn(b, e);
+		});
+	for (auto &x : th) x.join();
 }
 
 static int make_part(const host_csr &csr, int device, std::shared_ptr<gpu_part> &out)
 {
+	if (csr.ncols > (1ull << 30))
+		return set_error(FMX_ERR_UNSUPPORTED, "%llu columns: the entry stream holds 30-bit column ids",
+				(unsigned long long)csr.ncols);
 	auto p = std::make_shared<gpu_part>();
 	p->device = device;
 	p->nrows = csr.nrows; p->ncols = csr.ncols; p->nnz = csr.nnz;
 	p->prim = csr.prim; p->esize = csr.esize;
-
-	// schedule
 	const uint64_t n = csr.nrows;
-	std::vector<int32_t> light;
-	std::vector<split_task> heavy_tasks, medium_tasks;
-	std::vector<heavy_row> heavy;
-	light.reserve(n);
-	uint32_t slots = 0;
-	std::vector<uint32_t> bucket_count(kLightMax + 2);
-	std::vector<int32_t> band_rows;
-	for (uint64_t b0 = 0; b0 < n; b0 += kBand) {
-		uint64_t b1 = std::min<uint64_t>(n, b0 + kBand);
-		std::fill(bucket_count.begin(), bucket_count.end(), 0);
-		for (uint64_t r = b0; r < b1; r++) {
-			uint32_t d = csr.row_ptr[r + 1] - csr.row_ptr[r];
-			if (d <= kLightMax) bucket_count[kLightMax - d + 1]++;
+	const size_t es = csr.esize;
+
+	// hot columns: the highest in-degrees (at least 2), up to kHotMax
+	std::vector<std::atomic<uint32_t>> indeg(csr.ncols);
+	par_for(csr.ncols, [&](uint64_t b, uint64_t e) { for (uint64_t i = b; i < e; i++) indeg[i].store(0, std::memory_order_relaxed); });
+	par_for(csr.nnz, [&](uint64_t b, uint64_t e) {
+		for (uint64_t i = b; i < e; i++) indeg[csr.col[i]].fetch_add(1, std::memory_order_relaxed);
+	});
+	std::vector<int32_t> hot_col;
+	std::vector<int32_t> slot_of(csr.ncols, -1);
+	{
+		// counting sort of the columns by in-degree, descending, capped
+		const uint32_t cap = 1u << 16;
+		std::vector<uint64_t> cnt(cap + 2, 0);
+		for (uint64_t c = 0; c < csr.ncols; c++) {
+			uint32_t d = std::min(indeg[c].load(std::memory_order_relaxed), cap);
+			if (d >= 2) cnt[cap - d + 1]++;
 		}
-		// counting sort by degree, descending, stable by row
-		for (uint32_t i = 1; i < bucket_count.size(); i++) bucket_count[i] += bucket_count[i - 1];
-		band_rows.assign(bucket_count.back(), 0);
-		for (uint64_t r = b0; r < b1; r++) {
-			uint32_t d = csr.row_ptr[r + 1] - csr.row_ptr[r];
-			if (d <= kLightMax) band_rows[bucket_count[kLightMax - d]++] = int32_t(r);
-			else if (d <= kHeavyMin) medium_tasks.push_back({int32_t(r), csr.row_ptr[r], csr.row_ptr[r + 1], -1});
-			else {
-				uint32_t cnt = (d + kChunk - 1) / kChunk;
-				heavy.push_back({int32_t(r), slots, cnt});
-				for (uint32_t c = 0; c < cnt; c++) {
-					uint32_t s = csr.row_ptr[r] + c * kChunk;
-					uint32_t e = std::min(csr.row_ptr[r + 1], s + kChunk);
-					heavy_tasks.push_back({int32_t(r), s, e, int32_t(slots + c)});
+		for (size_t i = 1; i < cnt.size(); i++) cnt[i] += cnt[i - 1];
+		const uint64_t nhot = std::min<uint64_t>(kHotMax, cnt.back());
+		std::vector<int32_t> order(cnt.back());
+		for (uint64_t c = 0; c < csr.ncols; c++) {
+			uint32_t d = std::min(indeg[c].load(std::memory_order_relaxed), cap);
+			if (d >= 2) order[cnt[cap - d]++] = int32_t(c);
+		}
+		hot_col.assign(order.begin(), order.begin() + nhot);
+		// slot 0 is the zero row; hot columns take slots 1..nhot
+		for (uint64_t s = 0; s < nhot; s++) slot_of[hot_col[s]] = int32_t(s + 1);
+	}
+
+	// Work segments: runs of consecutive rows (every row in order; an exact
+	// row with its entries, an empty or longer row as one zero-row entry),
+	// then the equal chunks of the longer rows.  Each segment starts at a
+	// multiple of kStep in the stream and is padded to one.
+	const uint32_t zero_entry = 0u | kHot;          // slot 0: the zero row
+	struct seg_t { uint64_t row0, row1; uint32_t b, e; uint32_t slot; uint64_t at; uint32_t len; };
+	std::vector<seg_t> segs;
+	std::vector<heavy_row> heavy;
+	uint32_t n_exact = 0;
+	{
+		uint64_t run = 0;                        // real entries in the open run
+		for (uint64_t r = 0; r < n; r++) {
+			const uint32_t d = csr.row_ptr[r + 1] - csr.row_ptr[r];
+			const uint32_t len = (d >= 1 && d <= kExactMax) ? d : 1;
+			n_exact += (d >= 1 && d <= kExactMax);
+			if (segs.empty() || run >= kRange) {
+				segs.push_back({r, r + 1, 0, 0, kNoSlot, 0, 0});
+				run = 0;
+			} else {
+				segs.back().row1 = r + 1;
+			}
+			run += len;
+			segs.back().len += len;
+		}
+	}
+	uint32_t slots = 0;
+	for (uint64_t r = 0; r < n; r++) {
+		const uint32_t d = csr.row_ptr[r + 1] - csr.row_ptr[r];
+		if (d <= kExactMax) continue;
+		const uint32_t cnt = (d + kChunk - 1) / kChunk;   // equal chunks of <= kChunk entries
+		heavy.push_back({int32_t(r), slots, cnt});
+		for (uint32_t c = 0; c < cnt; c++) {
+			const uint32_t b = uint32_t(uint64_t(d) * c / cnt), e = uint32_t(uint64_t(d) * (c + 1) / cnt);
+			segs.push_back({r, r + 1, b, e, slots + c, 0, e - b});
+		}
+		slots += cnt;
+	}
+	uint64_t total = 0;
+	for (auto &g : segs) {
+		g.at = total;
+		g.len = (g.len + kStep - 1) / kStep * kStep;
+		total += g.len;
+	}
+	if (total >= (1ull << 32) - 64)
+		return set_error(FMX_ERR_UNSUPPORTED, "%llu stream entries: offsets are 32-bit", (unsigned long long)total);
+	std::vector<range_t> ranges(segs.size());
+	for (size_t i = 0; i < segs.size(); i++)
+		ranges[i] = {uint32_t(segs[i].at), segs[i].len, uint32_t(segs[i].row0), segs[i].slot};
+	// largest ranges first, so that round-robin assignment balances the groups
+	std::stable_sort(ranges.begin(), ranges.end(), [](const range_t &x, const range_t &y) {
+		return x.len > y.len;
+	});
+
+	// the entry stream (plus kStep entries so that index prefetches stay in bounds)
+	const size_t padded = total + kStep;
+	std::vector<uint32_t> col(total, zero_entry);
+	std::vector<char> val(total * es, 0);
+	std::atomic<uint64_t> hot_entries{0};
+	auto put = [&](uint64_t r, uint32_t b, uint32_t e, uint64_t at) {
+		const uint32_t rb = csr.row_ptr[r];
+		uint64_t h = 0;
+		for (uint32_t i = b; i < e; i++) {
+			const uint32_t c = uint32_t(csr.col[rb + i]);
+			const int32_t sl = slot_of[c];
+			col[at + (i - b)] = sl >= 0 ? (uint32_t(sl) | kHot) : c;
+			h += sl >= 0;
+		}
+		if (es) memcpy(&val[at * es], &csr.val[size_t(rb + b) * es], size_t(e - b) * es);
+		return h;
+	};
+	par_for(segs.size(), [&](uint64_t sb, uint64_t se) {
+		uint64_t h = 0;
+		for (uint64_t i = sb; i < se; i++) {
+			const seg_t &g = segs[i];
+			if (g.slot != kNoSlot) { h += put(g.row0, g.b, g.e, g.at); continue; }
+			uint64_t at = g.at;
+			for (uint64_t r = g.row0; r < g.row1; r++) {
+				const uint32_t d = csr.row_ptr[r + 1] - csr.row_ptr[r];
+				if (d >= 1 && d <= kExactMax) {
+					h += put(r, 0, d, at);
+					at += d;
+				} else {
+					at += 1;                 // the zero-row entry already there
 				}
-				slots += cnt;
+				col[at - 1] |= kEnd;
 			}
 		}
-		light.insert(light.end(), band_rows.begin(), band_rows.end());
-	}
-	std::stable_sort(medium_tasks.begin(), medium_tasks.end(), [](const split_task &x, const split_task &y) {
-		return (x.end - x.start) > (y.end - y.start);
+		hot_entries += h;
 	});
-	std::vector<split_task> tasks;
-	tasks.reserve(heavy_tasks.size() + medium_tasks.size());
-	tasks.insert(tasks.end(), heavy_tasks.begin(), heavy_tasks.end());
-	tasks.insert(tasks.end(), medium_tasks.begin(), medium_tasks.end());
+	p->hot_entries = hot_entries.load();
 
 	int cur = 0;
 	cudaGetDevice(&cur);
 	CUDA_TRY(cudaSetDevice(device));
 	int rc = FMX_OK;
 	uint64_t &bytes = p->bytes;
-	rc = upload(&p->row_ptr, csr.row_ptr.data(), csr.row_ptr.size(), bytes);
-	if (!rc) rc = upload(&p->col, csr.col.data(), csr.col.size(), bytes);
-	if (!rc && csr.esize) {
+	rc = upload(&p->col, col.data(), col.size(), bytes, padded);
+	if (!rc && es) {
 		char *v = nullptr;
-		rc = upload(&v, csr.val.data(), csr.val.size(), bytes);
+		rc = upload(&v, val.data(), val.size(), bytes, padded * es);
 		p->val = v;
 	}
-	if (!rc) rc = upload(&p->light, light.data(), light.size(), bytes);
-	if (!rc) rc = upload(&p->tasks, tasks.data(), tasks.size(), bytes);
+	if (!rc) rc = upload(&p->hot_col, hot_col.data(), hot_col.size(), bytes);
+	if (!rc) rc = upload(&p->ranges, ranges.data(), ranges.size(), bytes);
 	if (!rc) rc = upload(&p->heavy, heavy.data(), heavy.size(), bytes);
-	p->n_light = uint32_t(light.size());
-	p->n_tasks = uint32_t(tasks.size());
+	p->n_hot = uint32_t(hot_col.size());
+	p->n_exact = n_exact;
+	p->n_ranges = uint32_t(ranges.size());
 	p->n_heavy = uint32_t(heavy.size());
 	p->n_partials = slots;
-	if (!rc && slots) {
-		size_t sz = size_t(slots) * kPartialStride * 8;
-		cudaError_t e = cudaMalloc(&p->partial, sz);
+	auto scratch = [&](void **ptr, size_t sz, const char *what) {
+		if (rc || !sz) return;
+		cudaError_t e = cudaMalloc(ptr, sz);
 		if (e != cudaSuccess)
-			rc = set_error(FMX_ERR_OOM, "cudaMalloc of %zu partial bytes failed: %s", sz, cudaGetErrorString(e));
+			rc = set_error(FMX_ERR_OOM, "cudaMalloc of %zu %s bytes failed: %s", sz, what, cudaGetErrorString(e));
 		else bytes += sz;
-	}
+	};
+	scratch(&p->partial, size_t(slots) * kPartialStride * 8, "partial-sum");
+	scratch(&p->xhot, size_t(p->n_hot + 1) * kPanelBytes, "hot-pack");
+	if (!rc && cudaMemset(p->xhot, 0, size_t(p->n_hot + 1) * kPanelBytes) != cudaSuccess)
+		rc = set_error(FMX_ERR_CUDA, "clearing the hot pack failed");
 	cudaSetDevice(cur);
 	if (rc) return rc;
 	out = p;
@@ -492,20 +762,49 @@ static int make_part(const host_csr &csr, int device, std::shared_ptr<gpu_part> 
 // Host: launching
 // ---------------------------------------------------------------------------
 
+template <class K>
+static unsigned persistent_blocks(K kernel, int device)
+{
+	int sms = 0, per = 0;
+	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kThreads, 0);
+	return unsigned(std::max(1, sms) * std::max(1, per));
+}
+
+#ifndef FMX_SPMM_STEP
+#define FMX_SPMM_STEP 4                  // entries gathered per stream step (4 or 8)
+#endif
+
+template <class XT, class YT, class A, class WT, int VEC, int NV, bool SI, bool SO>
+static int launch_one(const gpu_part &p, const spmm_args &a, cudaStream_t st)
+{
+	auto kern = spmm_kernel<XT, YT, A, WT, VEC, NV, FMX_SPMM_STEP, SI, SO>;
+	static unsigned blocks[64] = {0};
+	unsigned &b = blocks[p.device & 63];
+	if (!b) b = persistent_blocks(kern, p.device);
+	kern<<<b, kThreads, 0, st>>>(a);
+	CUDA_TRY(cudaGetLastError());
+	return FMX_OK;
+}
+
 template <class XT, class YT, class A, class WT, int VEC, int NV>
 static int launch_t(const gpu_part &p, spmm_args a, bool sin, bool sout, cudaStream_t st)
 {
-	uint64_t warps = a.n_tasks + a.n_light_warps;
-	uint64_t blocks = (warps * 32 + kThreads - 1) / kThreads;
-	if (blocks) {
-		if (blocks > 0x7FFFFFFFULL) return set_error(FMX_ERR_UNSUPPORTED, "grid too large");
-		const dim3 grid{static_cast<unsigned>(blocks)};
-		if (sin && sout) spmm_kernel<XT, YT, A, WT, VEC, NV, true, true><<<grid, kThreads, 0, st>>>(a);
-		else if (sin) spmm_kernel<XT, YT, A, WT, VEC, NV, true, false><<<grid, kThreads, 0, st>>>(a);
-		else if (sout) spmm_kernel<XT, YT, A, WT, VEC, NV, false, true><<<grid, kThreads, 0, st>>>(a);
-		else spmm_kernel<XT, YT, A, WT, VEC, NV, false, false><<<grid, kThreads, 0, st>>>(a);
+	{
+		const uint64_t total = uint64_t(p.n_hot + 1) * a.k;
+		const unsigned pb = unsigned(std::min<uint64_t>((total + 255) / 256, 148ull * 16));
+		if (sin) pack_hot_kernel<XT, A, true><<<pb, 256, 0, st>>>(p.hot_col, p.n_hot, static_cast<const XT *>(a.X),
+				a.ldx, a.k, static_cast<XT *>(p.xhot), a.hot_ld, static_cast<const A *>(a.s_in));
+		else pack_hot_kernel<XT, A, false><<<pb, 256, 0, st>>>(p.hot_col, p.n_hot, static_cast<const XT *>(a.X),
+				a.ldx, a.k, static_cast<XT *>(p.xhot), a.hot_ld, nullptr);
 		CUDA_TRY(cudaGetLastError());
 	}
+	int rc;
+	if (sin && sout) rc = launch_one<XT, YT, A, WT, VEC, NV, true, true>(p, a, st);
+	else if (sin) rc = launch_one<XT, YT, A, WT, VEC, NV, true, false>(p, a, st);
+	else if (sout) rc = launch_one<XT, YT, A, WT, VEC, NV, false, true>(p, a, st);
+	else rc = launch_one<XT, YT, A, WT, VEC, NV, false, false>(p, a, st);
+	if (rc) return rc;
 	if (p.n_heavy) {
 		unsigned fb = unsigned((uint64_t(p.n_heavy) * 32 + 255) / 256);
 		if (sout) spmm_fixup_kernel<YT, A, true><<<fb, 256, 0, st>>>(p.heavy, p.n_heavy, static_cast<const A *>(a.partial),
@@ -519,32 +818,33 @@ static int launch_t(const gpu_part &p, spmm_args a, bool sin, bool sout, cudaStr
 
 static bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
 
-// Run one orientation over all column panels.
+// Run one orientation over all column panels (kPanelBytes of X row each).
 template <class XT, class YT, class A, class WT>
 static int run_typed(const gpu_part &p, const void *X, int64_t ldx, void *Y, int64_t ldy, int64_t k,
 		const void *sin, const void *sout, cudaStream_t st)
 {
 	constexpr int VEC = int(16 / sizeof(XT));
+	constexpr int kPanel = kPanelBytes / int(sizeof(XT));
 	// 16-byte vectors along k when every X and Y row starts 16-byte aligned
 	// and k is a multiple of VEC; otherwise scalar lanes.
 	const bool vec_ok = (k % VEC == 0) && (ldx % VEC == 0) && (ldy % VEC == 0) &&
 			aligned16(X) && aligned16(Y) && (VEC * sizeof(YT)) % 8 == 0;
-	const int64_t panel = vec_ok ? int64_t(32) * VEC : 128;
-	for (int64_t c0 = 0; c0 < k; c0 += panel) {
-		const int kp = int(std::min<int64_t>(panel, k - c0));
+	for (int64_t c0 = 0; c0 < k; c0 += kPanel) {
+		const int kp = int(std::min<int64_t>(kPanel, k - c0));
 		spmm_args a{};
-		a.row_ptr = p.row_ptr; a.col = p.col; a.val = p.val; a.light = p.light; a.tasks = p.tasks;
+		a.col = p.col; a.val = p.val; a.ranges = p.ranges;
 		a.X = static_cast<const XT *>(X) + c0;
+		a.xhot = p.xhot;
+		a.hot_ld = kp;                // packed rows back to back (two 64-byte rows per line)
 		a.Y = static_cast<YT *>(Y) + c0;
 		a.s_in = sin; a.s_out = sout; a.partial = p.partial;
 		a.ldx = ldx; a.ldy = ldy; a.k = kp;
-		a.n_light = p.n_light; a.n_tasks = p.n_tasks;
+		a.n_ranges = p.n_ranges;
 		int rc;
 		if (vec_ok) {
-			a.G = kp / VEC;           // <= 32
+			a.G = kp / VEC;           // <= 8
 			a.R = 32 / a.G;
 			a.nv = 1;
-			a.n_light_warps = (uint64_t(p.n_light) + a.R - 1) / a.R;
 			rc = launch_t<XT, YT, A, WT, VEC, 1>(p, a, sin, sout, st);
 		} else {
 			int g = 1;
@@ -552,7 +852,6 @@ static int run_typed(const gpu_part &p, const void *X, int64_t ldx, void *Y, int
 			a.G = g;
 			a.R = 32 / g;
 			a.nv = (kp + g - 1) / g;   // <= 4
-			a.n_light_warps = (uint64_t(p.n_light) + a.R - 1) / a.R;
 			rc = launch_t<XT, YT, A, WT, 1, 4>(p, a, sin, sout, st);
 		}
 		if (rc) return rc;
@@ -842,15 +1141,25 @@ int fmx_spmm_host(const fmx_matrix *m, int x_type, const void *X_host, int64_t l
 	return rc;
 }
 
+int fmx_matrix_hot(const fmx_matrix *m, uint64_t *n_hot_cols, uint64_t *hot_entries, uint64_t *scratch_bytes)
+{
+	if (!m || !m->a) return set_error(FMX_ERR_INVAL, "null matrix");
+	const gpu_part &p = *m->a;
+	if (n_hot_cols) *n_hot_cols = p.n_hot;
+	if (hot_entries) *hot_entries = p.hot_entries;
+	if (scratch_bytes) *scratch_bytes = uint64_t(p.n_hot + 1) * kPanelBytes + uint64_t(p.n_partials) * kPartialStride * 8;
+	return FMX_OK;
+}
+
 int fmx_matrix_schedule(const fmx_matrix *m, uint64_t *n_light_rows, uint64_t *n_split_tasks,
 		uint64_t *n_heavy_rows, uint64_t *kernels_per_spmm)
 {
 	if (!m || !m->a) return set_error(FMX_ERR_INVAL, "null matrix");
 	const gpu_part &p = *m->a;
-	if (n_light_rows) *n_light_rows = p.n_light;
-	if (n_split_tasks) *n_split_tasks = p.n_tasks;
+	if (n_light_rows) *n_light_rows = p.n_exact;
+	if (n_split_tasks) *n_split_tasks = p.n_ranges;
 	if (n_heavy_rows) *n_heavy_rows = p.n_heavy;
-	if (kernels_per_spmm) *kernels_per_spmm = 1 + (p.n_heavy ? 1 : 0);
+	if (kernels_per_spmm) *kernels_per_spmm = 2 + (p.n_heavy ? 1 : 0);
 	return FMX_OK;
 }
 

@@ -238,6 +238,12 @@ class sparse_matrix:
         check(lib.fmx_matrix_schedule(self._h, *[C.byref(x) for x in v]))
         return tuple(x.value for x in v)
 
+    def hot(self):
+        """(hot columns packed per SpMM, entries reading the pack, scratch bytes)."""
+        v = [C.c_uint64() for _ in range(3)]
+        check(lib.fmx_matrix_hot(self._h, *[C.byref(x) for x in v]))
+        return tuple(x.value for x in v)
+
     def transpose(self):
         h = C.c_void_p()
         check(lib.fmx_matrix_transpose(self._h, C.byref(h)))

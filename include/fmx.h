@@ -145,6 +145,10 @@ int fmx_matrix_free(fmx_matrix *m);
  * Each output row is summed in ascending column order by one lane group, the
  * reference's order, except rows longer than the split threshold, which are
  * summed as fixed-order partial chunks.  Asynchronous on `stream`. */
+/* Rows with at most this many entries are summed by one lane group in the
+ * reference's order; their results are bit-identical to the reference's. */
+#define FMX_EXACT_ROW_MAX 256
+
 int fmx_spmm(const fmx_matrix *m, int x_type, const void *X, int64_t ldx,
              int y_type, void *Y, int64_t ldy, int64_t k,
              const void *row_scale_in, const void *row_scale_out, void *stream);
@@ -155,10 +159,17 @@ int fmx_spmm_host(const fmx_matrix *m, int x_type, const void *X_host, int64_t l
                   int y_type, void *Y_host, int64_t ldy, int64_t k);
 
 /* Work decomposition of the resident matrix: rows summed by one lane group,
- * warp tasks (long rows and chunks of very long rows), rows finished by the
- * chunk-sum pass, and kernel launches per 128-column panel of one fmx_spmm. */
+ * work ranges (runs of whole rows, or chunks of rows longer than
+ * FMX_EXACT_ROW_MAX), rows finished by the chunk-sum pass, and kernel
+ * launches per 128-byte column panel of one fmx_spmm. */
 int fmx_matrix_schedule(const fmx_matrix *m, uint64_t *n_light_rows, uint64_t *n_split_tasks,
                         uint64_t *n_heavy_rows, uint64_t *kernels_per_spmm);
+
+/* Hot-column pack of the resident matrix: columns whose X rows each SpMM
+ * packs into scratch (the highest in-degrees, up to 2^20), the entries that
+ * read the pack, and the scratch bytes held (pack + long-row partial sums). */
+int fmx_matrix_hot(const fmx_matrix *m, uint64_t *n_hot_cols, uint64_t *hot_entries,
+                   uint64_t *scratch_bytes);
 
 /* ---- synthetic graphs ---------------------------------------------------------
  * R-MAT edges (a,b,c; d = 1-a-b-c) of 2^scale vertices, counter-based so the
