@@ -1197,3 +1197,123 @@ int fmx_rmat_edges_device(int scale, uint64_t nedges, double a, double b, double
 }
 
 } // extern "C"
+
+// ---------------------------------------------------------------------------
+// SpMM that allocates nothing
+//
+// For callers that cannot allocate device memory while they run: code inside
+// a memory pool or arena that owns all of the device's memory, code running
+// where the allocator is off limits (a custom allocator's own callbacks, a
+// signal-driven or real-time path), or hosts that forbid device allocation
+// after start-up.  fmx_spmm itself allocates nothing per call either, but its
+// scratch is allocated with the matrix; this entry point instead uses a fixed
+// scratch array compiled into the library, so its scratch exists on every
+// GPU that loads libfmx from load until process exit.
+// ---------------------------------------------------------------------------
+namespace fmx {
+
+constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;     // 32 MiB per device
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+static std::mutex g_noalloc_mu;
+static void *g_noalloc_ptr[64];
+
+// The device address of the scratch array on `device` (the current device).
+// Host code cannot use g_noalloc_scratch directly: there it is only a host
+// stand-in for the symbol, not a device address.
+static int noalloc_scratch(int device, void **ptr)
+{
+	if (device < 0 || device >= 64) return set_error(FMX_ERR_UNSUPPORTED, "device %d out of range for the fixed scratch", device);
+	std::lock_guard<std::mutex> g(g_noalloc_mu);
+	if (!g_noalloc_ptr[device]) {
+		void *p = nullptr;
+		cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+		if (e != cudaSuccess || !p)
+			return set_error(FMX_ERR_CUDA, "cudaGetSymbolAddress of the fixed scratch failed: %s", cudaGetErrorString(e));
+		g_noalloc_ptr[device] = p;
+	}
+	*ptr = g_noalloc_ptr[device];
+	return FMX_OK;
+}
+
+template <class WT>
+static int run_noalloc(const gpu_part &p, const float *X, int64_t ldx, float *Y, int64_t ldy, int64_t k,
+		void *xhot, void *partial, cudaStream_t st)
+{
+	constexpr int VEC = 4;
+	constexpr int kPanel = kPanelBytes / int(sizeof(float));
+	const bool vec_ok = (k % VEC == 0) && (ldx % VEC == 0) && (ldy % VEC == 0) && aligned16(X) && aligned16(Y);
+	for (int64_t c0 = 0; c0 < k; c0 += kPanel) {
+		const int kp = int(std::min<int64_t>(kPanel, k - c0));
+		spmm_args a{};
+		a.col = p.col; a.val = p.val; a.ranges = p.ranges;
+		a.X = X + c0;
+		a.xhot = xhot;
+		a.hot_ld = kp;
+		a.Y = Y + c0;
+		a.partial = partial;
+		a.ldx = ldx; a.ldy = ldy; a.k = kp;
+		a.n_ranges = p.n_ranges;
+		const uint64_t total = uint64_t(p.n_hot + 1) * kp;
+		const unsigned pb = unsigned(std::min<uint64_t>((total + 255) / 256, 148ull * 16));
+		pack_hot_kernel<float, float, false><<<pb, 256, 0, st>>>(p.hot_col, p.n_hot, X + c0, ldx, kp,
+				static_cast<float *>(xhot), kp, nullptr);
+		CUDA_TRY(cudaGetLastError());
+		int rc;
+		if (vec_ok) {
+			a.G = kp / VEC;
+			a.R = 32 / a.G;
+			a.nv = 1;
+			rc = launch_one<float, float, float, WT, VEC, 1, false, false>(p, a, st);
+		} else {
+			int g = 1;
+			while (g < 32 && g * 4 < kp) g *= 2;
+			a.G = g;
+			a.R = 32 / g;
+			a.nv = (kp + g - 1) / g;
+			rc = launch_one<float, float, float, WT, 1, 4, false, false>(p, a, st);
+		}
+		if (rc) return rc;
+		if (p.n_heavy) {
+			unsigned fb = unsigned((uint64_t(p.n_heavy) * 32 + 255) / 256);
+			spmm_fixup_kernel<float, float, false><<<fb, 256, 0, st>>>(p.heavy, p.n_heavy,
+					static_cast<const float *>(partial), Y + c0, ldy, kp, nullptr);
+			CUDA_TRY(cudaGetLastError());
+		}
+	}
+	return FMX_OK;
+}
+
+} // namespace fmx
+
+extern "C" int fmx_spmm_noalloc(const fmx_matrix *m, const float *X, int64_t ldx, float *Y, int64_t ldy,
+		int64_t k, void *stream)
+{
+	using namespace fmx;
+	if (!m || !m->a || !X || !Y) return set_error(FMX_ERR_INVAL, "null argument");
+	const gpu_part &p = *m->a;
+	if (k <= 0 || ldx < k || ldy < k) return set_error(FMX_ERR_DIM, "bad k (%lld) or leading dimensions", (long long)k);
+	if (p.prim != FMX_P_BOOL && p.prim != FMX_P_FLOAT)
+		return set_error(FMX_ERR_TYPE, "fmx_spmm_noalloc takes binary or float-weighted matrices");
+	// scratch layout: the hot pack (widest panel), then the long-row partial sums
+	const size_t hot_bytes = (size_t(p.n_hot + 1) * kPanelBytes + 255) / 256 * 256;
+	const size_t need = hot_bytes + size_t(p.n_partials) * kPartialStride * sizeof(float);
+	if (need > kNoAllocScratchBytes)
+		return set_error(FMX_ERR_UNSUPPORTED, "this matrix needs %zu bytes of SpMM scratch; the fixed scratch of "
+				"fmx_spmm_noalloc holds %zu bytes (use fmx_spmm)", need, kNoAllocScratchBytes);
+	int cur = 0;
+	cudaGetDevice(&cur);
+	if (cur != p.device && cudaSetDevice(p.device) != cudaSuccess)
+		return set_error(FMX_ERR_CUDA, "cannot select device %d", p.device);
+	void *base = nullptr;
+	int rc = noalloc_scratch(p.device, &base);
+	if (!rc) {
+		void *xhot = base;
+		void *partial = static_cast<char *>(base) + hot_bytes;
+		cudaStream_t st = static_cast<cudaStream_t>(stream);
+		rc = (p.prim == FMX_P_BOOL) ? run_noalloc<void>(p, X, ldx, Y, ldy, k, xhot, partial, st)
+		                            : run_noalloc<float>(p, X, ldx, Y, ldy, k, xhot, partial, st);
+	}
+	if (cur != p.device) cudaSetDevice(cur);
+	return rc;
+}

@@ -153,6 +153,22 @@ int fmx_spmm(const fmx_matrix *m, int x_type, const void *X, int64_t ldx,
              int y_type, void *Y, int64_t ldy, int64_t k,
              const void *row_scale_in, const void *row_scale_out, void *stream);
 
+/* FP32 SpMM that allocates nothing (no counterpart in the reference).
+ * For callers that must not allocate device memory while they run: code
+ * inside a memory pool or arena that owns the device's memory, allocator
+ * callbacks, real-time or signal-driven paths.  Same arguments and results as
+ * fmx_spmm with x_type = y_type = FMX_F32 and no row scales, for binary or
+ * float-weighted matrices.  Its scratch is one fixed 32 MiB array compiled
+ * into libfmx, present on every GPU that loads the library until the process
+ * exits; matrices whose SpMM scratch (fmx_matrix_hot) exceeds 32 MiB are
+ * rejected with FMX_ERR_UNSUPPORTED.  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress), so make that first call
+ * before any stream capture.  All calls share the array: calls that overlap on
+ * the GPU (on different streams, or from different threads) race and must not
+ * be issued. */
+int fmx_spmm_noalloc(const fmx_matrix *m, const float *X, int64_t ldx, float *Y,
+                     int64_t ldy, int64_t k, void *stream);
+
 /* Host-buffer SpMM: copies X in and Y out through the device (pinned or
  * pageable host memory), synchronous.  The e2e path a CPU caller uses. */
 int fmx_spmm_host(const fmx_matrix *m, int x_type, const void *X_host, int64_t ldx,
