@@ -70,7 +70,10 @@ namespace fmx {
 constexpr uint32_t kExactMax = FMX_EXACT_ROW_MAX;  // rows summed by one lane group
 constexpr uint32_t kChunk = 256;        // most entries per chunk of a longer row
 constexpr uint32_t kRange = 256;        // target entries per multi-row range
-constexpr uint32_t kHotMax = 1u << 20;  // most packed hot columns
+#ifndef FMX_HOT_MAX
+#define FMX_HOT_MAX (1u << 20)
+#endif
+constexpr uint32_t kHotMax = FMX_HOT_MAX;  // most packed hot columns
 constexpr int kPanelBytes = 128;        // X row bytes per panel (hot pack row)
 constexpr int kPartialStride = 256;     // AccT slots per partial (one panel)
 constexpr int kThreads = 256;           // threads per SpMM block
@@ -287,6 +290,22 @@ __device__ __forceinline__ xvec<T, VEC> ld_x_hint(const T *p, uint64_t pol)
 	return r;
 }
 
+// Store one 16-byte vector when `pred` holds, without a branch (a predicated
+// streaming store); other widths fall back to a guarded plain store.
+template <class T, int VEC>
+__device__ __forceinline__ void st_y_if(T *p, const T (&v)[VEC], bool pred)
+{
+	if constexpr (VEC * sizeof(T) == 16) {
+		uint32_t u[4];
+		memcpy(u, v, 16);
+		asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %5, 0;\n\t"
+				"@q st.global.cs.v4.u32 [%0], {%1,%2,%3,%4};\n\t}"
+				:: "l"(p), "r"(u[0]), "r"(u[1]), "r"(u[2]), "r"(u[3]), "r"(uint32_t(pred)) : "memory");
+	} else {
+		if (pred) st_y<T, VEC>(p, v);
+	}
+}
+
 struct spmm_args {
 	const uint32_t *col;
 	const void *val;
@@ -461,10 +480,15 @@ __device__ __forceinline__ void run_range(const spmm_args &a, const range_t rg, 
 			const bool hot = raw[u] & kHot;
 			const XT *xr = (hot ? H : X) + int64_t(c) * (hot ? int64_t(a.hot_ld) : a.ldx) + colbase;
 			const uint64_t pol = hot ? pol_hot : pol_cold;
+			if constexpr (NV == 1) {
+				// 16-byte lanes: every lane of a group owns a valid vector
+				x[u][0] = ld_x_hint<XT, VEC>(xr, pol);
+			} else {
 #pragma unroll
-			for (int v = 0; v < NV; v++)
-				if (v < a.nv && colbase + v * stride < a.k)
-					x[u][v] = ld_x_hint<XT, VEC>(xr + v * stride, pol);
+				for (int v = 0; v < NV; v++)
+					if (v < a.nv && colbase + v * stride < a.k)
+						x[u][v] = ld_x_hint<XT, VEC>(xr + v * stride, pol);
+			}
 			if constexpr (SCALE_IN) sc[u] = hot ? A(1) : static_cast<const A *>(a.s_in)[c];
 			ends |= (raw[u] >> 31) << u;
 		}
@@ -475,7 +499,7 @@ __device__ __forceinline__ void run_range(const spmm_args &a, const range_t rg, 
 		for (int u = 0; u < U; u++) {
 #pragma unroll
 			for (int v = 0; v < NV; v++)
-				if (v < a.nv && colbase + v * stride < a.k) {
+				if (NV == 1 || (v < a.nv && colbase + v * stride < a.k)) {
 					// (x * s_in) * w, rounded per step like scale_rows then SpMM;
 					// for hot entries x * s_in was rounded by the pack
 					if constexpr (SCALE_IN && !kBinary) acc.template add<XT, 2>(v, x[u][v], sc[u], w[u]);
@@ -484,7 +508,22 @@ __device__ __forceinline__ void run_range(const spmm_args &a, const range_t rg, 
 					else acc.template add<XT, 0>(v, x[u][v], A(1), A(1));
 				}
 			const bool end = runs && ((ends >> u) & 1u);
-			if (end) store_row<YT, A, VEC, NV, SCALE_OUT>(a, int32_t(row), colbase, acc);
+			if constexpr (NV == 1) {
+				// branch-free row close: predicated store, select-reset
+				YT *Yp = static_cast<YT *>(a.Y) + int64_t(row) * a.ldy + colbase;
+				A so = A(1);
+				if constexpr (SCALE_OUT) so = end ? static_cast<const A *>(a.s_out)[row] : A(1);
+				YT out[VEC];
+#pragma unroll
+				for (int i = 0; i < VEC; i++) {
+					A t = acc.get(0, i);
+					if constexpr (SCALE_OUT) t = acc_mul(t, so);
+					out[i] = from_acc<YT, A>(t);
+				}
+				st_y_if<YT, VEC>(Yp, out, end);
+			} else {
+				if (end) store_row<YT, A, VEC, NV, SCALE_OUT>(a, int32_t(row), colbase, acc);
+			}
 			acc.zero_if(end);
 			row += end;
 		}
