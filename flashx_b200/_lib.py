@@ -24,6 +24,8 @@ P_BOOL, P_INTEGER, P_LONG, P_FLOAT, P_DOUBLE = 0, 4, 6, 8, 9
 
 EXACT_ROW_MAX = 256   # FMX_EXACT_ROW_MAX: rows summed in the reference's order
 
+DENSE_BF16, DENSE_TF32X3, DENSE_F64 = 0, 1, 2
+
 BUILD_DEDUP = 0x1
 BUILD_KEEP_SELF_LOOPS = 0x2
 BUILD_REF_VALUE_LAYOUT = 0x4
@@ -71,6 +73,11 @@ _SIGS = {
     "fmx_spmm_noalloc": (_int, [_vp, _vp, _i64, _vp, _i64, _i64, _vp]),
     "fmx_matrix_schedule": (_int, [_vp, _P(_u64), _P(_u64), _P(_u64), _P(_u64)]),
     "fmx_matrix_hot": (_int, [_vp, _P(_u64), _P(_u64), _P(_u64)]),
+    "fmx_dense_gemm": (_int, [_int, _vp, _i64, _i64, _int, _vp, _int, _int, _vp, _i64, _vp, _vp]),
+    "fmx_dense_gram_parts": (_int, [_int, _i64]),
+    "fmx_dense_gram": (_int, [_int, _vp, _i64, _int, _vp, _i64, _int, _i64, _vp, _vp, _vp, _vp]),
+    "fmx_dense_chol_inv": (_int, [_vp, _int, _vp, _vp, _vp]),
+    "fmx_dense_sym_eig": (_int, [_vp, _int, _vp, _vp, _vp]),
     "fmx_rmat_edges_host": (_int, [_int, _u64, _d, _d, _d, _u64, _int, _vp, _vp, _int]),
     "fmx_rmat_edges_device": (_int, [_int, _u64, _d, _d, _d, _u64, _int, _vp, _vp, _vp]),
 }

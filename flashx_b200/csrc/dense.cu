@@ -1,0 +1,713 @@
+// Dense kernels of the block eigensolver (the FlashMatrix eigensolver's
+// dense products: block_multi_vector::MvTransMv / gemm / MvNorm,
+// matrix/eigensolver/block_dense_matrix.cpp:997-1530, FM_MultiVector.h:389-676).
+//
+// Tall-skinny operands: X is n x K (n in the millions, K <= 64), row-major.
+//
+//  tc_gemm   Y = X B           (basis update; B is K x N, small)
+//  tc_gram   G = X^T W         (projection; W is n x N; MN-major operands for
+//                               BF16, K-major (staged transposed) for TF32)
+//     on the 5th-generation tensor cores: tcgen05.mma with the operands staged
+//     in shared memory by the CTA's threads and the 128 x N FP32 accumulator
+//     in tensor memory (TMEM), read back with tcgen05.ld.  Two precisions:
+//       BF16   one MMA per K step, FP32 accumulate (early, loose iterations)
+//       TF32x3 x = hi + lo split (hi = tf32(x), lo = tf32(x - hi)); the
+//              products hi*hi + hi*lo + lo*hi reach FP32 accuracy
+//  gram_f64  G = X^T W in FP64 on the CUDA cores (Cholesky-QR, residuals)
+//  small FP64 kernels on one CTA: Cholesky factor inverse, Jacobi
+//  eigendecomposition (the projected Rayleigh-Ritz problem).
+//
+// Every mbarrier wait is bounded; a wait that runs out sets *err and the
+// kernel finishes without touching the result, so a hang cannot happen.
+#include "fmx_internal.h"
+
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+
+namespace fmx {
+int set_error(int code, const char *fmt, ...);
+}
+
+namespace fmx {
+namespace dense {
+
+#define DCUDA_TRY(call)                                                         \
+	do {                                                                        \
+		cudaError_t err__ = (call);                                             \
+		if (err__ != cudaSuccess)                                               \
+			return set_error(FMX_ERR_CUDA, "%s failed: %s (%s:%d)", #call,      \
+					cudaGetErrorString(err__), __FILE__, __LINE__);             \
+	} while (0)
+
+constexpr int kTile = 128;          // rows per tensor-core tile (MMA M)
+constexpr uint32_t kWaitPolls = 1u << 20;
+
+// ---------------------------------------------------------------------------
+// tcgen05 / mbarrier primitives (PTX ISA 8.6, sm_100a)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return uint32_t(__cvta_generic_to_shared(p)); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+	asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t phase)
+{
+	uint32_t ok;
+	asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+			"selp.u32 %0, 1, 0, p;\n\t}" : "=r"(ok) : "r"(smem_u32(bar)), "r"(phase) : "memory");
+	return ok != 0;
+}
+// Bounded wait: false when the phase did not complete in kWaitPolls polls.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t phase)
+{
+	for (uint32_t i = 0; i < kWaitPolls; i++)
+		if (mbar_try_wait(bar, phase)) return true;
+	return false;
+}
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_alloc(uint32_t *dst_smem, uint32_t ncols)
+{
+	asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+			:: "r"(smem_u32(dst_smem)), "r"(ncols) : "memory");
+	asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols)
+{
+	asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(taddr), "r"(ncols) : "memory");
+}
+
+// D(tmem) (+)= A(smem) * B(smem), one instruction, issued by one thread.
+template <bool TF32>
+__device__ __forceinline__ void umma(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t accumulate)
+{
+	const uint32_t m0 = 0, m1 = 0, m2 = 0, m3 = 0;
+	if constexpr (TF32)
+		asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+				"tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+				:: "r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate),
+				   "r"(m0), "r"(m1), "r"(m2), "r"(m3) : "memory");
+	else
+		asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+				"tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+				:: "r"(d_tmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate),
+				   "r"(m0), "r"(m1), "r"(m2), "r"(m3) : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint64_t *bar)
+{
+	asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+			:: "r"(smem_u32(bar)) : "memory");
+}
+// 32 lanes x 16 consecutive 32-bit columns: thread t of the warp gets lane t.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16])
+{
+	uint32_t r[16];
+	asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+			: "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+			  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+			: "r"(taddr) : "memory");
+	asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+	for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+// Shared-memory matrix descriptor, no swizzle (canonical "interleave"
+// layout of 8-row x 16-byte core matrices): start, leading and stride byte
+// offsets in 16-byte units, version 1 (sm100).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo_bytes, uint32_t sbo_bytes)
+{
+	uint64_t d = 0;
+	d |= uint64_t((addr >> 4) & 0x3FFF);
+	d |= uint64_t((lbo_bytes >> 4) & 0x3FFF) << 16;
+	d |= uint64_t((sbo_bytes >> 4) & 0x3FFF) << 32;
+	d |= uint64_t(1) << 46;                  // version
+	return d;                                // base offset 0, layout SWIZZLE_NONE (0)
+}
+// Instruction descriptor: FP32 accumulate, A/B format (1 = BF16, 2 = TF32),
+// majors (0 = K-major, 1 = MN-major), N, M = 128.
+__host__ __device__ constexpr uint32_t instr_desc(uint32_t fmt, uint32_t a_mn, uint32_t b_mn, uint32_t n)
+{
+	return (1u << 4) | (fmt << 7) | (fmt << 10) | (a_mn << 15) | (b_mn << 16) | ((n >> 3) << 17) | ((128u >> 4) << 24);
+}
+
+__device__ __forceinline__ float tf32_round(float x)
+{
+	uint32_t r;
+	asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+	return __uint_as_float(r);
+}
+
+// ---------------------------------------------------------------------------
+// Y (n x N) = X (n x K) B (K x N).  A = X tile (128 x Kp), K-major: 16-byte
+// K units, each unit holding all 128 rows back to back (LBO = 128 rows x 16 B,
+// SBO = 8 rows x 16 B).  B^T (N x Kp) in the same layout.  Kp = K padded to
+// the MMA K step (16 BF16 / 8 TF32 elements = 32 bytes).
+// ---------------------------------------------------------------------------
+template <bool TF32>
+struct gemm_cfg {
+	static constexpr int E = TF32 ? 4 : 8;        // elements per 16-byte unit
+	static constexpr int KSTEP = TF32 ? 8 : 16;   // elements per MMA
+	static constexpr int PARTS = TF32 ? 2 : 1;    // hi (+ lo)
+};
+
+template <bool TF32>
+__device__ __forceinline__ void put_units(char *base, int unit_stride, int row, const float *v, int K, int Kp, int part)
+{
+	// write row `row` of a K-major operand: units of E elements at base + u*unit_stride + row*16
+	constexpr int E = gemm_cfg<TF32>::E;
+	for (int u = 0; u < Kp / E; u++) {
+		uint32_t w[4];
+		if constexpr (TF32) {
+#pragma unroll
+			for (int i = 0; i < 4; i++) {
+				const int k = u * 4 + i;
+				const float x = k < K ? v[k] : 0.f;
+				const float hi = tf32_round(x);
+				w[i] = __float_as_uint(part == 0 ? hi : tf32_round(x - hi));
+			}
+		} else {
+#pragma unroll
+			for (int i = 0; i < 4; i++) {
+				const int k = u * 8 + 2 * i;
+				const float a = k < K ? v[k] : 0.f, b = k + 1 < K ? v[k + 1] : 0.f;
+				__nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+				memcpy(&w[i], &h, 4);
+			}
+		}
+		*reinterpret_cast<uint4 *>(base + size_t(u) * unit_stride + size_t(row) * 16) = make_uint4(w[0], w[1], w[2], w[3]);
+	}
+}
+
+template <bool TF32>
+__global__ void __launch_bounds__(128)
+tc_gemm_kernel(const float *__restrict__ X, int64_t ldx, int K, const float *__restrict__ B, int ldb, int N,
+		float *__restrict__ Y, int64_t ldy, int64_t n, int *err)
+{
+	using C = gemm_cfg<TF32>;
+	const int Kp = (K + C::KSTEP - 1) / C::KSTEP * C::KSTEP;
+	const int Np = (N + 15) / 16 * 16;                 // MMA N (multiple of 16 for M = 128)
+	extern __shared__ __align__(1024) char smem[];
+	const size_t a_bytes = size_t(Kp / C::E) * kTile * 16;
+	const size_t b_bytes = size_t(Kp / C::E) * Np * 16;
+	char *sa = smem;                                   // PARTS x a_bytes
+	char *sb = smem + C::PARTS * a_bytes;              // PARTS x b_bytes
+	__shared__ uint64_t bar;
+	__shared__ uint32_t tmem_base;
+	const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+	const uint32_t ncols = Np <= 32 ? 32 : (Np <= 64 ? 64 : 128);
+
+	// B^T once: row j of B^T = column j of B
+	for (int j = tid; j < Np; j += blockDim.x) {
+		float col[64];
+		for (int k = 0; k < Kp; k++) col[k] = (j < N && k < K) ? B[size_t(k) * ldb + j] : 0.f;
+		for (int part = 0; part < C::PARTS; part++)
+			put_units<TF32>(sb + part * b_bytes, Np * 16, j, col, Kp, Kp, part);
+	}
+	if (warp == 0) tmem_alloc(&tmem_base, ncols);
+	if (tid == 0) { mbar_init(&bar, 1); asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+	fence_async_smem();
+	tc_fence_before();
+	__syncthreads();
+	tc_fence_after();
+	const uint32_t tmem = tmem_base;
+	const uint32_t idesc = instr_desc(TF32 ? 2 : 1, 0, 0, uint32_t(Np));
+	uint32_t phase = 0;
+	bool ok = true;
+	const int64_t ntiles = (n + kTile - 1) / kTile;
+	for (int64_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+		const int64_t row = t * kTile + tid;
+		float v[64];
+		for (int k = 0; k < Kp; k++) v[k] = (row < n && k < K) ? X[row * ldx + k] : 0.f;
+		for (int part = 0; part < C::PARTS; part++)
+			put_units<TF32>(sa + part * a_bytes, kTile * 16, tid, v, Kp, Kp, part);
+		fence_async_smem();
+		__syncthreads();
+		if (tid == 0) {
+			tc_fence_after();
+			uint32_t acc = 0;
+			// passes: (hi, hi), then for TF32 (hi, lo) and (lo, hi)
+			const int npass = TF32 ? 3 : 1;
+			for (int pass = 0; pass < npass; pass++) {
+				const int pa = (pass == 2) ? 1 : 0, pb = (pass == 1) ? 1 : 0;
+				for (int s = 0; s < Kp / C::KSTEP; s++) {
+					const uint32_t a_addr = smem_u32(sa + pa * a_bytes) + uint32_t(s) * 2 * kTile * 16;
+					const uint32_t b_addr = smem_u32(sb + pb * b_bytes) + uint32_t(s) * 2 * Np * 16;
+					umma<TF32>(tmem, smem_desc(a_addr, kTile * 16, 128), smem_desc(b_addr, Np * 16, 128), idesc, acc);
+					acc = 1;
+				}
+			}
+			umma_commit(&bar);
+		}
+		__syncwarp();
+		ok = __syncthreads_and(mbar_wait(&bar, phase));
+		phase ^= 1;
+		tc_fence_after();
+		if (ok) {
+			// warp w reads TMEM lanes 32w..32w+31 = tile rows 32w..32w+31
+			const int64_t r = t * kTile + warp * 32 + lane;
+			for (int c0 = 0; c0 < Np; c0 += 16) {
+				float o[16];
+				tmem_ld16(tmem + (uint32_t(warp * 32) << 16) + uint32_t(c0), o);
+				if (r < n)
+					for (int i = 0; i < 16 && c0 + i < N; i++) Y[r * ldy + c0 + i] = o[i];
+			}
+		}
+		tc_fence_before();
+		__syncthreads();
+	}
+	if (!ok && tid == 0) atomicExch(err, 1);
+	__syncthreads();
+	if (warp == 0) tmem_dealloc(tmem, ncols);
+}
+
+// ---------------------------------------------------------------------------
+// G (M x N) = X^T W over row chunks of 128: A = X^T chunk and B = W chunk are
+// MN-major (rows of X and W are contiguous along M and N).  Core matrix =
+// 8 chunk rows x 16 bytes; LBO = 128 B between 8-row groups, SBO = 16 groups
+// x 128 B between 16-byte units along M (or N).  M is padded to 128 with zero
+// units.  Each CTA leaves its partial in part[blockIdx.x]; gram_reduce adds
+// the partials in CTA order.
+// ---------------------------------------------------------------------------
+template <bool TF32>
+__device__ __forceinline__ void put_mn_row(char *base, int krow, const float *v, int M, int Mp, int part)
+{
+	constexpr int E = TF32 ? 4 : 8;
+	for (int u = 0; u < Mp / E; u++) {
+		uint32_t w[4];
+		if constexpr (TF32) {
+#pragma unroll
+			for (int i = 0; i < 4; i++) {
+				const int m = u * 4 + i;
+				const float x = m < M ? v[m] : 0.f;
+				const float hi = tf32_round(x);
+				w[i] = __float_as_uint(part == 0 ? hi : tf32_round(x - hi));
+			}
+		} else {
+#pragma unroll
+			for (int i = 0; i < 4; i++) {
+				const int m = u * 8 + 2 * i;
+				__nv_bfloat162 h = __floats2bfloat162_rn(m < M ? v[m] : 0.f, m + 1 < M ? v[m + 1] : 0.f);
+				memcpy(&w[i], &h, 4);
+			}
+		}
+		*reinterpret_cast<uint4 *>(base + size_t(u) * 2048 + size_t(krow >> 3) * 128 + size_t(krow & 7) * 16) =
+				make_uint4(w[0], w[1], w[2], w[3]);
+	}
+}
+
+// K-major operand of the Gram for TF32: column m of the chunk (K = the
+// chunk's rows) as 16-byte units of 4 rows; unit (k / 4) of row m lives at
+// base + (k / 4) * ustride + m * 16 + (k % 4) * 4.  Rows m >= M stay zero.
+__device__ __forceinline__ void put_k_col(char *base, int ustride, int krow, const float *v, int M, int part)
+{
+	for (int m = 0; m < M; m++) {
+		const float x = v[m];
+		const float hi = tf32_round(x);
+		*reinterpret_cast<float *>(base + size_t(krow >> 2) * ustride + size_t(m) * 16 + size_t(krow & 3) * 4) =
+				part == 0 ? hi : tf32_round(x - hi);
+	}
+}
+
+template <bool TF32>
+__global__ void __launch_bounds__(128)
+tc_gram_kernel(const float *__restrict__ X, int64_t ldx, int M, const float *__restrict__ W, int64_t ldw, int N,
+		int64_t n, float *__restrict__ part, int *err)
+{
+	// BF16: MN-major operands (rows of X and W copied as they are).
+	// TF32: K-major operands (X^T and W^T, written transposed).
+	constexpr int E = TF32 ? 4 : 8;
+	constexpr int KSTEP = TF32 ? 8 : 16;             // chunk rows per MMA
+	constexpr int PARTS = TF32 ? 2 : 1;
+	const int Np = (N + 15) / 16 * 16;
+	extern __shared__ __align__(1024) char smem[];
+	const size_t a_bytes = TF32 ? size_t(kTile / 4) * kTile * 16 : size_t(kTile / E) * 2048;  // M padded to 128
+	const size_t b_bytes = TF32 ? size_t(kTile / 4) * Np * 16 : size_t(Np / E) * 2048;
+	char *sa = smem, *sb = smem + PARTS * a_bytes;
+	__shared__ uint64_t bar;
+	__shared__ uint32_t tmem_base;
+	const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+	const uint32_t ncols = Np <= 32 ? 32 : (Np <= 64 ? 64 : 128);
+	// zero the operands once: the padding (M rows or units beyond M, N) is
+	// never rewritten
+	for (size_t i = tid; i < (PARTS * (a_bytes + b_bytes)) / 16; i += blockDim.x)
+		reinterpret_cast<uint4 *>(sa)[i] = make_uint4(0, 0, 0, 0);
+	if (warp == 0) tmem_alloc(&tmem_base, ncols);
+	if (tid == 0) { mbar_init(&bar, 1); asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+	tc_fence_before();
+	__syncthreads();
+	tc_fence_after();
+	const uint32_t tmem = tmem_base;
+	const uint32_t idesc = TF32 ? instr_desc(2, 0, 0, uint32_t(Np)) : instr_desc(1, 1, 1, uint32_t(Np));
+	const int Mp = (M + E - 1) / E * E;
+	uint32_t phase = 0;
+	uint32_t acc = 0;
+	bool ok = true;
+	const int64_t nchunks = (n + kTile - 1) / kTile;
+	for (int64_t c = blockIdx.x; c < nchunks && ok; c += gridDim.x) {
+		const int64_t row = c * kTile + tid;
+		float v[64];
+		for (int m = 0; m < Mp; m++) v[m] = (row < n && m < M) ? X[row * ldx + m] : 0.f;
+		if constexpr (TF32) {
+			for (int p = 0; p < PARTS; p++) put_k_col(sa + p * a_bytes, kTile * 16, tid, v, M, p);
+		} else {
+			put_mn_row<false>(sa, tid, v, M, Mp, 0);
+		}
+		for (int j = 0; j < Np; j++) v[j] = (row < n && j < N) ? W[row * ldw + j] : 0.f;
+		if constexpr (TF32) {
+			for (int p = 0; p < PARTS; p++) put_k_col(sb + p * b_bytes, Np * 16, tid, v, N, p);
+		} else {
+			put_mn_row<false>(sb, tid, v, N, Np, 0);
+		}
+		fence_async_smem();
+		__syncthreads();
+		if (tid == 0) {
+			tc_fence_after();
+			const int npass = TF32 ? 3 : 1;
+			for (int pass = 0; pass < npass; pass++) {
+				const int pa = (pass == 2) ? 1 : 0, pb = (pass == 1) ? 1 : 0;
+				for (int s = 0; s < kTile / KSTEP; s++) {
+					if constexpr (TF32) {
+						// K-major: 8 chunk rows = 2 units; LBO = unit stride, SBO = 8 rows x 16 B
+						const uint32_t a_addr = smem_u32(sa + pa * a_bytes) + uint32_t(s) * 2 * kTile * 16;
+						const uint32_t b_addr = smem_u32(sb + pb * b_bytes) + uint32_t(s) * 2 * Np * 16;
+						umma<true>(tmem, smem_desc(a_addr, kTile * 16, 128), smem_desc(b_addr, Np * 16, 128), idesc, acc);
+					} else {
+						// MN-major: 16 chunk rows = 2 groups of 128 bytes; LBO = group
+						// stride, SBO = 16-byte unit stride along M (N)
+						const uint32_t off = uint32_t(s) * 2 * 128;
+						umma<false>(tmem, smem_desc(smem_u32(sa) + off, 128, 2048), smem_desc(smem_u32(sb) + off, 128, 2048),
+								idesc, acc);
+					}
+					acc = 1;
+				}
+			}
+			umma_commit(&bar);
+		}
+		__syncwarp();
+		ok = __syncthreads_and(mbar_wait(&bar, phase));
+		phase ^= 1;
+		tc_fence_after();
+		tc_fence_before();
+		__syncthreads();                           // operands free for the next chunk
+	}
+	// rows 0..M-1 of D: warp w holds rows 32w..32w+31.  The condition must be
+	// the same for every thread: tcgen05.ld is a warp-collective instruction.
+	const bool had_chunks = int64_t(blockIdx.x) < nchunks;
+	if (ok && had_chunks) {
+		const int r = warp * 32 + lane;
+		for (int c0 = 0; c0 < Np; c0 += 16) {
+			float o[16];
+			tmem_ld16(tmem + (uint32_t(warp * 32) << 16) + uint32_t(c0), o);
+			if (r < M)
+				for (int i = 0; i < 16 && c0 + i < N; i++) part[(size_t(blockIdx.x) * M + r) * N + c0 + i] = o[i];
+		}
+	} else if (ok) {
+		for (int i = tid; i < M * N; i += blockDim.x) part[size_t(blockIdx.x) * M * N + i] = 0.f;
+	}
+	if (!ok && tid == 0) atomicExch(err, 1);
+	tc_fence_before();
+	__syncthreads();
+	tc_fence_after();
+	if (warp == 0) tmem_dealloc(tmem, ncols);
+}
+
+template <class T>
+__global__ void gram_reduce_kernel(const T *part, int nparts, int MN, T *G)
+{
+	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < MN; i += gridDim.x * blockDim.x) {
+		T s = 0;
+		for (int p = 0; p < nparts; p++) s += part[size_t(p) * MN + i];
+		G[i] = s;
+	}
+}
+
+// ---------------------------------------------------------------------------
+// FP64 Gram on CUDA cores: part[cta] = sum over the CTA's rows of x^T w (FP64)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+gram_f64_kernel(const float *__restrict__ X, int64_t ldx, int M, const float *__restrict__ W, int64_t ldw, int N,
+		int64_t n, double *__restrict__ part)
+{
+	__shared__ float sx[64][65], sw[64][65];
+	const int tid = threadIdx.x;
+	const int pairs = M * N;
+	double acc[16];
+#pragma unroll
+	for (int q = 0; q < 16; q++) acc[q] = 0;
+	for (int64_t r0 = int64_t(blockIdx.x) * 64; r0 < n; r0 += int64_t(gridDim.x) * 64) {
+		for (int i = tid; i < 64 * 64; i += 256) {
+			const int rr = i / 64, cc = i % 64;
+			const int64_t row = r0 + rr;
+			sx[rr][cc] = (row < n && cc < M) ? X[row * ldx + cc] : 0.f;
+			sw[rr][cc] = (row < n && cc < N) ? W[row * ldw + cc] : 0.f;
+		}
+		__syncthreads();
+#pragma unroll
+		for (int q = 0; q < 16; q++) {
+			const int p = tid + q * 256;
+			if (p < pairs) {
+				const int i = p / N, j = p % N;
+				double s = 0;
+				for (int rr = 0; rr < 64; rr++) s += double(sx[rr][i]) * double(sw[rr][j]);
+				acc[q] += s;
+			}
+		}
+		__syncthreads();
+	}
+#pragma unroll
+	for (int q = 0; q < 16; q++) {
+		const int p = tid + q * 256;
+		if (p < pairs) part[size_t(blockIdx.x) * pairs + p] = acc[q];
+	}
+}
+
+// ---------------------------------------------------------------------------
+// Small FP64 problems on one CTA (b <= 64)
+// ---------------------------------------------------------------------------
+
+// T = R^{-1} with G = R^T R (upper Cholesky).  info = 0, or the 1-based
+// column whose pivot was not positive.  One CTA of 64 threads.
+__global__ void chol_inv_kernel(const double *__restrict__ G, int b, double *__restrict__ T, int *info)
+{
+	extern __shared__ double dyn[];                  // two 64 x 65 FP64 matrices
+	double (*R)[65] = reinterpret_cast<double (*)[65]>(dyn);
+	double (*Ti)[65] = reinterpret_cast<double (*)[65]>(dyn + 64 * 65);
+	const int t = threadIdx.x;
+	for (int i = t; i < b * b; i += blockDim.x) R[i / b][i % b] = G[i];
+	__syncthreads();
+	__shared__ int bad;
+	if (t == 0) bad = 0;
+	__syncthreads();
+	for (int k = 0; k < b; k++) {
+		if (t == 0) {
+			double d = R[k][k];
+			for (int p = 0; p < k; p++) d -= R[p][k] * R[p][k];
+			if (!(d > 0) && !bad) bad = k + 1;
+			R[k][k] = d > 0 ? sqrt(d) : 1.0;
+		}
+		__syncthreads();
+		for (int j = k + 1 + t; j < b; j += blockDim.x) {
+			double s = R[k][j];
+			for (int p = 0; p < k; p++) s -= R[p][k] * R[p][j];
+			R[k][j] = s / R[k][k];
+		}
+		__syncthreads();
+	}
+	// inverse of the upper-triangular R, column by column
+	for (int j = t; j < b; j += blockDim.x) {
+		for (int i = b - 1; i >= 0; i--) {
+			if (i > j) { Ti[i][j] = 0; continue; }
+			double s = (i == j) ? 1.0 : 0.0;
+			for (int p = i + 1; p <= j; p++) s -= R[i][p] * Ti[p][j];
+			Ti[i][j] = s / R[i][i];
+		}
+	}
+	__syncthreads();
+	for (int i = t; i < b * b; i += blockDim.x) T[i] = Ti[i / b][i % b];
+	if (t == 0) *info = bad;
+}
+
+// Symmetric eigendecomposition H = V diag(w) V^T by cyclic Jacobi rotations
+// (round-robin pairs, b/2 rotations in parallel per step).  Eigenvalues in
+// descending order, V columns matching.  One CTA of 32 threads.
+__global__ void jacobi_eig_kernel(const double *__restrict__ H, int b, double *__restrict__ w, double *__restrict__ V,
+		int max_sweeps)
+{
+	extern __shared__ double dyn[];                  // two 64 x 65 FP64 matrices
+	double (*A)[65] = reinterpret_cast<double (*)[65]>(dyn);
+	double (*Q)[65] = reinterpret_cast<double (*)[65]>(dyn + 64 * 65);
+	__shared__ int pr[32], pc[32];
+	__shared__ double cs[32], sn[32];
+	__shared__ int order[64];
+	__shared__ double off;
+	const int t = threadIdx.x;
+	const int m = (b + 1) & ~1;                       // even size (pad with a zero row/column)
+	for (int i = t; i < m * m; i += blockDim.x) {
+		const int r = i / m, c = i % m;
+		A[r][c] = (r < b && c < b) ? 0.5 * (H[r * b + c] + H[c * b + r]) : 0.0;
+		Q[r][c] = (r == c) ? 1.0 : 0.0;
+	}
+	__syncthreads();
+	for (int sweep = 0; sweep < max_sweeps; sweep++) {
+		if (t == 0) {
+			double s = 0, d = 0;
+			for (int r = 0; r < m; r++)
+				for (int c = 0; c < m; c++) (r == c ? d : s) += A[r][c] * A[r][c];
+			off = s / (d > 0 ? d : 1.0);
+		}
+		__syncthreads();
+		if (off < 1e-30) break;
+		for (int step = 0; step < m - 1; step++) {
+			// round-robin tournament pairing of 0..m-1
+			if (t < m / 2) {
+				int a = t == 0 ? 0 : 1 + (t - 1 + step) % (m - 1);
+				int bb = 1 + (m - 2 - t + step) % (m - 1);
+				if (a > bb) { int x = a; a = bb; bb = x; }
+				pr[t] = a; pc[t] = bb;
+				const double app = A[a][a], aqq = A[bb][bb], apq = A[a][bb];
+				double c = 1, s = 0;
+				if (fabs(apq) > 1e-300) {
+					const double tau = (aqq - app) / (2 * apq);
+					const double tt = (tau >= 0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1 + tau * tau));
+					c = 1 / sqrt(1 + tt * tt);
+					s = tt * c;
+				}
+				cs[t] = c; sn[t] = s;
+			}
+			__syncthreads();
+			// rows: A <- J^T A
+			for (int k = t; k < m; k += blockDim.x)
+				for (int q = 0; q < m / 2; q++) {
+					const int p0 = pr[q], p1 = pc[q];
+					const double x = A[p0][k], y = A[p1][k];
+					A[p0][k] = cs[q] * x - sn[q] * y;
+					A[p1][k] = sn[q] * x + cs[q] * y;
+				}
+			__syncthreads();
+			// columns: A <- A J, Q <- Q J
+			for (int k = t; k < m; k += blockDim.x)
+				for (int q = 0; q < m / 2; q++) {
+					const int p0 = pr[q], p1 = pc[q];
+					double x = A[k][p0], y = A[k][p1];
+					A[k][p0] = cs[q] * x - sn[q] * y;
+					A[k][p1] = sn[q] * x + cs[q] * y;
+					x = Q[k][p0]; y = Q[k][p1];
+					Q[k][p0] = cs[q] * x - sn[q] * y;
+					Q[k][p1] = sn[q] * x + cs[q] * y;
+				}
+			__syncthreads();
+		}
+	}
+	if (t == 0) {
+		// descending order of the b real eigenvalues (the padding one, if any, is dropped)
+		int idx[64];
+		int cnt = 0;
+		for (int i = 0; i < m; i++) {
+			bool pad = (m != b) && (fabs(Q[b][i]) > 0.5);   // eigenvector of the zero padding
+			if (!pad && cnt < b) idx[cnt++] = i;
+		}
+		for (int i = 0; i < cnt; i++)
+			for (int j = i + 1; j < cnt; j++)
+				if (A[idx[j]][idx[j]] > A[idx[i]][idx[i]]) { int x = idx[i]; idx[i] = idx[j]; idx[j] = x; }
+		for (int i = 0; i < cnt; i++) order[i] = idx[i];
+	}
+	__syncthreads();
+	for (int i = t; i < b; i += blockDim.x) w[i] = A[order[i]][order[i]];
+	for (int i = t; i < b * b; i += blockDim.x) V[i] = Q[i / b][order[i % b]];
+}
+
+int sms(int device)
+{
+	int s = 0;
+	cudaDeviceGetAttribute(&s, cudaDevAttrMultiProcessorCount, device);
+	return s > 0 ? s : 1;
+}
+
+} // namespace dense
+} // namespace fmx
+
+using namespace fmx;
+using namespace fmx::dense;
+
+extern "C" {
+
+int fmx_dense_gemm(int precision, const float *X, int64_t ldx, int64_t n, int K, const float *B, int ldb, int N,
+		float *Y, int64_t ldy, int *err, void *stream)
+{
+	if (!X || !B || !Y || !err) return set_error(FMX_ERR_INVAL, "null argument");
+	if (K < 1 || K > 64 || N < 1 || N > 64) return set_error(FMX_ERR_UNSUPPORTED, "tensor-core GEMM takes K, N in 1..64");
+	if (precision != FMX_DENSE_BF16 && precision != FMX_DENSE_TF32X3)
+		return set_error(FMX_ERR_INVAL, "unknown precision %d", precision);
+	const bool tf32 = precision == FMX_DENSE_TF32X3;
+	const int E = tf32 ? 4 : 8, KSTEP = tf32 ? 8 : 16, parts = tf32 ? 2 : 1;
+	const int Kp = (K + KSTEP - 1) / KSTEP * KSTEP, Np = (N + 15) / 16 * 16;
+	const size_t smem = size_t(parts) * (size_t(Kp / E) * kTile * 16 + size_t(Kp / E) * Np * 16);
+	int dev = 0;
+	cudaGetDevice(&dev);
+	const int64_t tiles = (n + kTile - 1) / kTile;
+	const unsigned grid = unsigned(std::max<int64_t>(1, std::min<int64_t>(tiles, int64_t(sms(dev)) * 4)));
+	cudaStream_t st = static_cast<cudaStream_t>(stream);
+	if (tf32) {
+		DCUDA_TRY(cudaFuncSetAttribute(tc_gemm_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+		tc_gemm_kernel<true><<<grid, 128, smem, st>>>(X, ldx, K, B, ldb, N, Y, ldy, n, err);
+	} else {
+		DCUDA_TRY(cudaFuncSetAttribute(tc_gemm_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+		tc_gemm_kernel<false><<<grid, 128, smem, st>>>(X, ldx, K, B, ldb, N, Y, ldy, n, err);
+	}
+	DCUDA_TRY(cudaGetLastError());
+	return FMX_OK;
+}
+
+int fmx_dense_gram_parts(int precision, int64_t n)
+{
+	int dev = 0;
+	cudaGetDevice(&dev);
+	const int64_t chunks = (n + kTile - 1) / kTile;
+	if (precision == FMX_DENSE_F64) return int(std::max<int64_t>(1, std::min<int64_t>((n + 63) / 64, int64_t(sms(dev)) * 4)));
+	return int(std::max<int64_t>(1, std::min<int64_t>(chunks, int64_t(sms(dev)) * (precision == FMX_DENSE_TF32X3 ? 1 : 2))));
+}
+
+int fmx_dense_gram(int precision, const float *X, int64_t ldx, int M, const float *W, int64_t ldw, int N, int64_t n,
+		void *part, void *G, int *err, void *stream)
+{
+	if (!X || !W || !part || !G) return set_error(FMX_ERR_INVAL, "null argument");
+	if (M < 1 || M > 64 || N < 1 || N > 64) return set_error(FMX_ERR_UNSUPPORTED, "Gram takes M, N in 1..64");
+	cudaStream_t st = static_cast<cudaStream_t>(stream);
+	const int parts = fmx_dense_gram_parts(precision, n);
+	if (precision == FMX_DENSE_F64) {
+		gram_f64_kernel<<<parts, 256, 0, st>>>(X, ldx, M, W, ldw, N, n, static_cast<double *>(part));
+		DCUDA_TRY(cudaGetLastError());
+		gram_reduce_kernel<double><<<(M * N + 255) / 256, 256, 0, st>>>(static_cast<const double *>(part), parts, M * N,
+				static_cast<double *>(G));
+		DCUDA_TRY(cudaGetLastError());
+		return FMX_OK;
+	}
+	if (!err) return set_error(FMX_ERR_INVAL, "null error flag");
+	const bool tf32 = precision == FMX_DENSE_TF32X3;
+	if (!tf32 && precision != FMX_DENSE_BF16) return set_error(FMX_ERR_INVAL, "unknown precision %d", precision);
+	const int Np = (N + 15) / 16 * 16;
+	const size_t smem = tf32 ? size_t(2) * (size_t(kTile / 4) * kTile * 16 + size_t(kTile / 4) * Np * 16)
+	                         : size_t(kTile / 8) * 2048 + size_t(Np / 8) * 2048;
+	if (tf32) {
+		DCUDA_TRY(cudaFuncSetAttribute(tc_gram_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+		tc_gram_kernel<true><<<parts, 128, smem, st>>>(X, ldx, M, W, ldw, N, n, static_cast<float *>(part), err);
+	} else {
+		DCUDA_TRY(cudaFuncSetAttribute(tc_gram_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+		tc_gram_kernel<false><<<parts, 128, smem, st>>>(X, ldx, M, W, ldw, N, n, static_cast<float *>(part), err);
+	}
+	DCUDA_TRY(cudaGetLastError());
+	gram_reduce_kernel<float><<<(M * N + 255) / 256, 256, 0, st>>>(static_cast<const float *>(part), parts, M * N,
+			static_cast<float *>(G));
+	DCUDA_TRY(cudaGetLastError());
+	return FMX_OK;
+}
+
+int fmx_dense_chol_inv(const double *G, int b, double *T, int *info, void *stream)
+{
+	if (!G || !T || !info) return set_error(FMX_ERR_INVAL, "null argument");
+	if (b < 1 || b > 64) return set_error(FMX_ERR_UNSUPPORTED, "b in 1..64");
+	const int smem = 2 * 64 * 65 * int(sizeof(double));
+	DCUDA_TRY(cudaFuncSetAttribute(chol_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+	chol_inv_kernel<<<1, 64, smem, static_cast<cudaStream_t>(stream)>>>(G, b, T, info);
+	DCUDA_TRY(cudaGetLastError());
+	return FMX_OK;
+}
+
+int fmx_dense_sym_eig(const double *H, int b, double *w, double *V, void *stream)
+{
+	if (!H || !w || !V) return set_error(FMX_ERR_INVAL, "null argument");
+	if (b < 1 || b > 64) return set_error(FMX_ERR_UNSUPPORTED, "b in 1..64");
+	const int smem = 2 * 64 * 65 * int(sizeof(double));
+	DCUDA_TRY(cudaFuncSetAttribute(jacobi_eig_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+	jacobi_eig_kernel<<<1, 32, smem, static_cast<cudaStream_t>(stream)>>>(H, b, w, V, 30);
+	DCUDA_TRY(cudaGetLastError());
+	return FMX_OK;
+}
+
+} // extern "C"

@@ -187,6 +187,37 @@ int fmx_matrix_schedule(const fmx_matrix *m, uint64_t *n_light_rows, uint64_t *n
 int fmx_matrix_hot(const fmx_matrix *m, uint64_t *n_hot_cols, uint64_t *hot_entries,
                    uint64_t *scratch_bytes);
 
+/* ---- dense kernels of the block eigensolver --------------------------------
+ * Tall-skinny products over n-row, row-major FP32 blocks of at most 64
+ * columns (block_multi_vector::gemm / MvTransMv / MvNorm,
+ * matrix/eigensolver/block_dense_matrix.cpp:997-1530).  Precision:
+ *   FMX_DENSE_BF16    tensor cores (tcgen05), BF16 operands, FP32 accumulate
+ *   FMX_DENSE_TF32X3  tensor cores, each operand split x = hi + lo in TF32 and
+ *                     hi*hi + hi*lo + lo*hi accumulated in FP32 (FP32 accuracy)
+ *   FMX_DENSE_F64     CUDA cores, FP64 accumulate (Gram only)
+ * `err` (device int) is set to 1 if a tensor-core wait ran out of time. */
+#define FMX_DENSE_BF16 0
+#define FMX_DENSE_TF32X3 1
+#define FMX_DENSE_F64 2
+
+/* Y (n x N) = X (n x K) * B (K x N); K, N <= 64; B row-major (ldb). */
+int fmx_dense_gemm(int precision, const float *X, int64_t ldx, int64_t n, int K,
+                   const float *B, int ldb, int N, float *Y, int64_t ldy, int *err,
+                   void *stream);
+/* Number of per-CTA partials the Gram of n rows uses (size of `part`:
+ * parts * M * N elements of float, or double for FMX_DENSE_F64). */
+int fmx_dense_gram_parts(int precision, int64_t n);
+/* G (M x N, row-major) = X^T W over n rows; float G, or double for F64.
+ * Partials are added in a fixed order (deterministic). */
+int fmx_dense_gram(int precision, const float *X, int64_t ldx, int M, const float *W,
+                   int64_t ldw, int N, int64_t n, void *part, void *G, int *err,
+                   void *stream);
+/* T = R^-1 where G = R^T R (upper Cholesky), FP64, b <= 64; *info = 0 or
+ * the 1-based column of the first non-positive pivot. */
+int fmx_dense_chol_inv(const double *G, int b, double *T, int *info, void *stream);
+/* H = V diag(w) V^T (symmetric, FP64, b <= 64), eigenvalues descending. */
+int fmx_dense_sym_eig(const double *H, int b, double *w, double *V, void *stream);
+
 /* ---- synthetic graphs ---------------------------------------------------------
  * R-MAT edges (a,b,c; d = 1-a-b-c) of 2^scale vertices, counter-based so the
  * host and device streams are identical.  `permute` relabels vertices by a
