@@ -201,11 +201,12 @@ def run_reference(a, rank, world):
     img, build_s = build_graph(a)
     nthreads, model = cpu_info()
     inf = img.info()
-    per = max(a.cpu_seconds / max(a.steps, 1), 0.5)
-    warm = min(a.warmup, 1)
-    for _ in range(warm):
-        cpu_sample(img, a, nthreads, per)
-    gbs, sample, times = cpu_sample(img, a, nthreads, per, reps=a.steps)
+    # each step is a bounded sample of the workload: the whole run (warm-up
+    # included) holds about 90 s of CPU work, at least one block row per step
+    warm = a.warmup
+    per = min(0.5, 90.0 / max(a.steps + warm, 1))
+    gbs, sample, times = cpu_sample(img, a, nthreads, per, reps=a.steps + warm)
+    gbs, times = gbs[warm:], times[warm:]
     value = float(np.median(gbs))
     line = {
         "metric": "SpMM GB/s (algorithmic bytes / time)", "value": round(value, 3), "unit": "GB/s",

@@ -236,3 +236,91 @@ def test_repeated_calls_varying_k(torch_cuda):
         X = rng.integers(-8, 9, (3000, k)).astype(np.float32)
         for _ in range(2):
             assert np.array_equal(_gpu_spmm(torch, m, X), oracle.spmm(idx, mat, X))
+
+
+def test_empty_matrix(torch_cuda):
+    """A matrix without edges (every block row stored as one empty tile) gives
+    Y = 0, overwriting whatever Y held."""
+    torch = torch_cuda
+    e = np.zeros(0, dtype=np.uint32)
+    idx, mat = oracle.build_image(e, e, None, nrows=64, ncols=64, block=(16, 16))
+    m = sparse_matrix.create(matrix_image.from_bytes(idx, mat), None)
+    assert m.get_nnz() == 0
+    for k in (1, 16):
+        X = np.ones((64, k), dtype=np.float32)
+        Y = _gpu_spmm(torch, m, X)
+        assert np.array_equal(Y, oracle.spmm(idx, mat, X)) and not Y.any()
+
+
+@pytest.fixture(scope="module")
+def rmat_s24():
+    """The bench graph: R-MAT scale 24, edge factor 16, seed 1, deduplicated,
+    self-loops removed, 16384 x 16384 tiles; unweighted and uniform(0,1]
+    weighted images of the same edges."""
+    src, dst = rmat_edges(24, seed=1)
+    n = 1 << 24
+    vals = np.random.default_rng(24).uniform(0.0, 1.0, len(src)).astype(np.float32)
+    vals[vals == 0] = 1.0
+    out = {}
+    for name, v in (("binary", None), ("weighted", vals)):
+        img = matrix_image.build(src, dst, v, nrows=n, ncols=n, block_size=(16384, 16384), dedup=True)
+        out[name] = img
+    del src, dst, vals
+    idx, mat = out["binary"].bytes()
+    rows, cols = oracle.nonzeros(idx, mat)
+    out["outdeg"] = np.bincount(rows.astype(np.int64), minlength=n)
+    out["indeg"] = np.bincount(cols.astype(np.int64), minlength=n)
+    return out
+
+
+@pytest.mark.parametrize("k", [1, 4, 16, 32])
+def test_rmat_s24_properties(torch_cuda, rmat_s24, k):
+    """Full-size checks on the bench graph, unweighted: A 1 = out-degrees;
+    A (X + Z) = A X + A Z bit for bit (integer-valued operands keep every
+    partial sum exact); the checksum of checksums 1^T (A X) = indeg^T X; and
+    bit-exact agreement with the oracle on a sample of block rows."""
+    torch = torch_cuda
+    img = rmat_s24["binary"]
+    m = sparse_matrix.create(img, None)
+    n = m.get_num_rows()
+    assert m.get_nnz() == int(rmat_s24["outdeg"].sum())
+    assert 8 * int(rmat_s24["outdeg"].max()) < (1 << 24)
+    ones = torch.ones((n, k), device="cuda")
+    y = torch.empty((n, k), device="cuda")
+    assert m.multiply(ones, y)
+    deg = torch.from_numpy(rmat_s24["outdeg"].astype(np.float32)).cuda()
+    assert torch.equal(y, deg[:, None].expand(n, k))
+    g = torch.Generator(device="cuda").manual_seed(k)
+    X = torch.randint(-4, 5, (n, k), generator=g, device="cuda").float()
+    Z = torch.randint(-4, 5, (n, k), generator=g, device="cuda").float()
+    yx, yz, ys = (torch.empty((n, k), device="cuda") for _ in range(3))
+    assert m.multiply(X, yx) and m.multiply(Z, yz) and m.multiply(X + Z, ys)
+    assert torch.equal(ys, yx + yz)
+    indeg = torch.from_numpy(rmat_s24["indeg"].astype(np.float64)).cuda()
+    assert torch.equal(yx.double().sum(0), (indeg[:, None] * X.double()).sum(0))
+    idx, mat = img.bytes()
+    Xh = X.cpu().numpy()
+    R = oracle.spmm(idx, mat, Xh, nthreads=16, brows=(0, 4))
+    assert np.array_equal(yx[: 4 * 16384].cpu().numpy(), R[: 4 * 16384])
+
+
+@pytest.mark.parametrize("k", [1, 16, 32])
+def test_rmat_s24_weighted(torch_cuda, rmat_s24, k):
+    """Full-size weighted image with N(0,1) operands: rows of at most
+    EXACT_ROW_MAX entries match the oracle bit for bit on a sample of block
+    rows, every sampled row within RTOL, and A 1 equals the oracle's row
+    sums of the weights within RTOL."""
+    torch = torch_cuda
+    img = rmat_s24["weighted"]
+    m = sparse_matrix.create(img, None)
+    n = m.get_num_rows()
+    g = torch.Generator(device="cuda").manual_seed(100 + k)
+    X = torch.randn((n, k), generator=g, device="cuda")
+    y = torch.empty((n, k), device="cuda")
+    assert m.multiply(X, y)
+    idx, mat = img.bytes()
+    R = oracle.spmm(idx, mat, X.cpu().numpy(), nthreads=16, brows=(0, 4))[: 4 * 16384]
+    Y = y[: 4 * 16384].cpu().numpy()
+    light = rmat_s24["outdeg"][: 4 * 16384] <= _lib.EXACT_ROW_MAX
+    assert np.array_equal(Y[light], R[light])
+    np.testing.assert_allclose(Y, R, rtol=RTOL, atol=RTOL * np.abs(R).max())
