@@ -26,6 +26,9 @@ EXACT_ROW_MAX = 256   # FMX_EXACT_ROW_MAX: rows summed in the reference's order
 
 DENSE_BF16, DENSE_TF32X3, DENSE_F64 = 0, 1, 2
 
+EIGEN_LA, EIGEN_LM = 0, 1
+EIGEN_PLAIN, EIGEN_MIXED = 0, 1
+
 BUILD_DEDUP = 0x1
 BUILD_KEEP_SELF_LOOPS = 0x2
 BUILD_REF_VALUE_LAYOUT = 0x4
@@ -49,6 +52,22 @@ lib = _load()
 
 _vp, _sz, _u64, _i64, _u32, _int, _d = C.c_void_p, C.c_size_t, C.c_uint64, C.c_int64, C.c_uint32, C.c_int, C.c_double
 _P = C.POINTER
+
+
+
+class eigen_options_t(C.Structure):
+    """struct fmx_eigen_options (include/fmx.h)."""
+    _fields_ = [("nev", C.c_int), ("block_size", C.c_int), ("degree", C.c_int), ("max_iters", C.c_int),
+                ("which", C.c_int), ("precision", C.c_int), ("tol", C.c_double), ("lower", C.c_double),
+                ("upper", C.c_double), ("bf16_until", C.c_double), ("seed", C.c_uint64), ("X0", C.c_void_p),
+                ("ldx0", C.c_int64)]
+
+
+class eigen_status_t(C.Structure):
+    """struct fmx_eigen_status (include/fmx.h)."""
+    _fields_ = [("iters", C.c_int), ("converged", C.c_int), ("num_ops", C.c_int64), ("spmm_calls", C.c_int64),
+                ("max_residual", C.c_double), ("seconds", C.c_double)]
+
 
 _SIGS = {
     "fmx_strerror": (C.c_char_p, [_int]),
@@ -78,6 +97,9 @@ _SIGS = {
     "fmx_dense_gram": (_int, [_int, _vp, _i64, _int, _vp, _i64, _int, _i64, _vp, _vp, _vp, _vp]),
     "fmx_dense_chol_inv": (_int, [_vp, _int, _vp, _vp, _vp]),
     "fmx_dense_sym_eig": (_int, [_vp, _int, _vp, _vp, _vp]),
+    "fmx_eigen_default_options": (None, [_P(eigen_options_t), _int]),
+    "fmx_eigen_solve": (_int, [_vp, _vp, _P(eigen_options_t), _vp, _vp, _i64, _vp, _P(eigen_status_t), _vp]),
+    "fmx_na_scale": (_int, [_vp, _vp, _vp]),
     "fmx_rmat_edges_host": (_int, [_int, _u64, _d, _d, _d, _u64, _int, _vp, _vp, _int]),
     "fmx_rmat_edges_device": (_int, [_int, _u64, _d, _d, _d, _u64, _int, _vp, _vp, _vp]),
 }

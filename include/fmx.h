@@ -218,6 +218,67 @@ int fmx_dense_chol_inv(const double *G, int b, double *T, int *info, void *strea
 /* H = V diag(w) V^T (symmetric, FP64, b <= 64), eigenvalues descending. */
 int fmx_dense_sym_eig(const double *H, int b, double *w, double *V, void *stream);
 
+/* ---- block eigensolver -------------------------------------------------------
+ * Largest eigenpairs of the symmetric operator diag(s) A diag(s) (s = NULL:
+ * A itself) by Chebyshev-filtered subspace iteration on a block of
+ * block_size vectors.  Replaces fm::eigen::compute_eigen
+ * (matrix/eigensolver/eigensolver.h:74-75, eigensolver.cpp:118-308); the
+ * option and status fields mirror eigen_options (eigensolver.h:59-73) and
+ * eigen_res::eigen_status (:51-54). */
+#define FMX_EIGEN_LA 0      /* largest algebraic ("LA") */
+#define FMX_EIGEN_LM 1      /* largest magnitude ("LM", the reference's default) */
+#define FMX_EIGEN_PLAIN 0   /* FP32 SpMM operands; dense products in FP64 on CUDA cores */
+#define FMX_EIGEN_MIXED 1   /* BF16 SpMM operands until bf16_until, then FP32; CholQR
+                               basis update and Rayleigh quotient on tensor cores
+                               (3xTF32); CholQR Gram, Cholesky, projected problem
+                               and residual norms in FP64 */
+
+typedef struct fmx_eigen_options {
+	int nev;            /* wanted eigenpairs (eigen_options::nev) */
+	int block_size;     /* vectors per block, nev <= block_size <= 64 */
+	int degree;         /* Chebyshev degree per filter pass (SpMMs per pass) */
+	int max_iters;      /* filter passes (eigen_options::max_iters) */
+	int which;          /* FMX_EIGEN_LA or FMX_EIGEN_LM (eigen_options::which) */
+	int precision;      /* FMX_EIGEN_PLAIN or FMX_EIGEN_MIXED */
+	double tol;         /* residual ||A x - l x|| / ||A|| every wanted pair must meet */
+	double lower;       /* lower bound of the spectrum (-1 for D^-1/2 A D^-1/2) */
+	double upper;       /* upper bound of the spectrum (1 for D^-1/2 A D^-1/2); ||A|| is
+	                       taken as max(|lower|, |upper|) */
+	double bf16_until;  /* FMX_EIGEN_MIXED: BF16 filter while the largest residual
+	                       exceeds this */
+	uint64_t seed;      /* random start block, uniform(-1, 1) (MvRandom) */
+	const float *X0;    /* optional start block on the device (n x block_size), or NULL */
+	int64_t ldx0;
+} fmx_eigen_options;
+
+typedef struct fmx_eigen_status {
+	int iters;          /* filter passes (eigen_status::num_iters) */
+	int converged;      /* wanted pairs whose explicit residual meets tol */
+	int64_t num_ops;    /* SpMM columns applied (eigen_status::num_ops) */
+	int64_t spmm_calls;
+	double max_residual;/* largest explicit residual of the wanted pairs */
+	double seconds;     /* wall time of the call */
+} fmx_eigen_status;
+
+/* Defaults as eigen_options() and init(nev) (eigensolver.cpp:82-116): tol 1e-8,
+ * max_iters 500, block_size max(2 nev, 16) (at most 64), degree 10, LA, plain,
+ * spectrum [-1, 1], seed 1. */
+void fmx_eigen_default_options(fmx_eigen_options *opts, int nev);
+
+/* Solve; evals and residuals are host arrays of nev, evecs a device array of
+ * n x nev (row-major, ldv), any of them NULL when not wanted.  The residuals
+ * are those of the returned vectors, from an explicit final product.  A run
+ * that stops at max_iters returns FMX_OK with status->converged < nev. */
+int fmx_eigen_solve(const fmx_matrix *m, const float *row_scale,
+                    const fmx_eigen_options *opts, double *evals, float *evecs,
+                    int64_t ldv, double *residuals, fmx_eigen_status *status,
+                    void *stream);
+
+/* s = D^-1/2 with D = A 1 (row sums; 0 where a row is empty), the scaling of
+ * NA_eigen_Operator (matrix/test/test-eigen.cpp:96-109); s is a device array
+ * of n floats. */
+int fmx_na_scale(const fmx_matrix *m, float *s, void *stream);
+
 /* ---- synthetic graphs ---------------------------------------------------------
  * R-MAT edges (a,b,c; d = 1-a-b-c) of 2^scale vertices, counter-based so the
  * host and device streams are identical.  `permute` relabels vertices by a

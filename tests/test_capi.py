@@ -69,3 +69,27 @@ def test_matrix_create_without_gpu_reports_cuda_error():
     rc = _lib.lib.fmx_matrix_create(img._h, None, 0, C.byref(h))
     assert rc == _lib.FMX_ERR_CUDA
     assert "device" in _lib.last_error()
+
+
+def test_eigen_structs_match_the_header(tmp_path):
+    """The ctypes mirrors of fmx_eigen_options / fmx_eigen_status have the C
+    layout, and fmx_eigen_default_options fills the reference's defaults
+    (eigen_options(), eigensolver.cpp:82-91) without touching a GPU."""
+    src = tmp_path / "s.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "fmx.h"\n'
+                   'int main(void) { printf("%zu %zu %zu %zu %zu\\n", sizeof(fmx_eigen_options),'
+                   ' offsetof(fmx_eigen_options, tol), offsetof(fmx_eigen_options, seed),'
+                   ' offsetof(fmx_eigen_options, ldx0), sizeof(fmx_eigen_status)); return 0; }\n')
+    exe = tmp_path / "s"
+    subprocess.run(["gcc", "-std=c99", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    O, S = _lib.eigen_options_t, _lib.eigen_status_t
+    assert got == [C.sizeof(O), O.tol.offset, O.seed.offset, O.ldx0.offset, C.sizeof(S)]
+    o = O()
+    _lib.lib.fmx_eigen_default_options(C.byref(o), 8)
+    assert (o.nev, o.block_size, o.max_iters, o.which, o.precision) == (8, 16, 500, _lib.EIGEN_LA, _lib.EIGEN_PLAIN)
+    assert o.tol == 1e-8 and (o.lower, o.upper) == (-1.0, 1.0)
+    from flashx_b200.eigen import eigen_options
+    e = eigen_options()
+    assert (e.tol, e.max_iters, e.which, e.max_restarts) == (1e-8, 500, "LM", 100)
+    assert e.init(8) and e.block_size == 16 and not e.init(8, "Lanczos")
