@@ -27,6 +27,7 @@ EXACT_ROW_MAX = 256   # FMX_EXACT_ROW_MAX: rows summed in the reference's order
 DENSE_BF16, DENSE_TF32X3, DENSE_F64 = 0, 1, 2
 
 EIGEN_LA, EIGEN_LM = 0, 1
+GNN_FEATURES, GNN_OUT, GNN_PARAMS = 64, 16, 5184
 EIGEN_PLAIN, EIGEN_MIXED = 0, 1
 
 BUILD_DEDUP = 0x1
@@ -59,7 +60,7 @@ class eigen_options_t(C.Structure):
     """struct fmx_eigen_options (include/fmx.h)."""
     _fields_ = [("nev", C.c_int), ("block_size", C.c_int), ("degree", C.c_int), ("max_iters", C.c_int),
                 ("which", C.c_int), ("precision", C.c_int), ("tol", C.c_double), ("lower", C.c_double),
-                ("upper", C.c_double), ("bf16_until", C.c_double), ("seed", C.c_uint64), ("X0", C.c_void_p),
+                ("upper", C.c_double), ("tensor_until", C.c_double), ("seed", C.c_uint64), ("X0", C.c_void_p),
                 ("ldx0", C.c_int64)]
 
 
@@ -100,6 +101,14 @@ _SIGS = {
     "fmx_eigen_default_options": (None, [_P(eigen_options_t), _int]),
     "fmx_eigen_solve": (_int, [_vp, _vp, _P(eigen_options_t), _vp, _vp, _i64, _vp, _P(eigen_status_t), _vp]),
     "fmx_na_scale": (_int, [_vp, _vp, _vp]),
+    "fmx_gnn_create": (_int, [_int, _u64, _P(_vp)]),
+    "fmx_gnn_free": (_int, [_vp]),
+    "fmx_gnn_set_params": (_int, [_vp, _vp]),
+    "fmx_gnn_get_params": (_int, [_vp, _vp]),
+    "fmx_gnn_features": (_int, [_vp, _vp, _u64, _vp, _vp]),
+    "fmx_gnn_forward": (_int, [_vp, _vp, _vp, _vp, _int, _vp, _vp]),
+    "fmx_gnn_loss_grad": (_int, [_vp, _vp, _vp, _vp, _vp, _i64, _int, _int, _vp, _vp, _vp]),
+    "fmx_gnn_adam_step": (_int, [_vp, C.c_float, _vp]),
     "fmx_rmat_edges_host": (_int, [_int, _u64, _d, _d, _d, _u64, _int, _vp, _vp, _int]),
     "fmx_rmat_edges_device": (_int, [_int, _u64, _d, _d, _d, _u64, _int, _vp, _vp, _vp]),
 }

@@ -429,41 +429,81 @@ __global__ void gram_reduce_kernel(const T *part, int nparts, int MN, T *G)
 
 // ---------------------------------------------------------------------------
 // FP64 Gram on CUDA cores: part[cta] = sum over the CTA's rows of x^T w (FP64)
+// Each thread owns a 4 x 4 block of G and every `groups`-th row: per row it
+// loads its 4 columns of x and of w straight from global memory (16-byte
+// loads when the leading dimensions allow, L1-shared by the threads of the
+// same row) and does 16 FP64 FMAs; four rows are in flight per thread.  The
+// row groups' blocks are added in a fixed order at the end (deterministic).
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ float4 ld4_guard(const float *p, int c, int lim, bool vec)
+{
+	if (vec && c + 3 < lim) return *reinterpret_cast<const float4 *>(p + c);
+	float4 v;
+	v.x = c < lim ? p[c] : 0.f;
+	v.y = c + 1 < lim ? p[c + 1] : 0.f;
+	v.z = c + 2 < lim ? p[c + 2] : 0.f;
+	v.w = c + 3 < lim ? p[c + 3] : 0.f;
+	return v;
+}
+
 __global__ void __launch_bounds__(256)
 gram_f64_kernel(const float *__restrict__ X, int64_t ldx, int M, const float *__restrict__ W, int64_t ldw, int N,
 		int64_t n, double *__restrict__ part)
 {
-	__shared__ float sx[64][65], sw[64][65];
+	__shared__ double red[256 * 16];
 	const int tid = threadIdx.x;
-	const int pairs = M * N;
-	double acc[16];
+	const int nbi = (M + 3) / 4, nbj = (N + 3) / 4, nblk = nbi * nbj;    // <= 256
+	const int groups = 256 / nblk;
+	const int blk = tid % nblk, grp = tid / nblk;
+	const int bi = blk / nbj, bj = blk % nbj;
+	const bool active = grp < groups;
+	const bool vx = (ldx % 4) == 0 && (reinterpret_cast<uintptr_t>(X) & 15) == 0;
+	const bool vw = (ldw % 4) == 0 && (reinterpret_cast<uintptr_t>(W) & 15) == 0;
+	double acc[4][4];
 #pragma unroll
-	for (int q = 0; q < 16; q++) acc[q] = 0;
-	for (int64_t r0 = int64_t(blockIdx.x) * 64; r0 < n; r0 += int64_t(gridDim.x) * 64) {
-		for (int i = tid; i < 64 * 64; i += 256) {
-			const int rr = i / 64, cc = i % 64;
-			const int64_t row = r0 + rr;
-			sx[rr][cc] = (row < n && cc < M) ? X[row * ldx + cc] : 0.f;
-			sw[rr][cc] = (row < n && cc < N) ? W[row * ldw + cc] : 0.f;
-		}
-		__syncthreads();
+	for (int a = 0; a < 4; a++)
 #pragma unroll
-		for (int q = 0; q < 16; q++) {
-			const int p = tid + q * 256;
-			if (p < pairs) {
-				const int i = p / N, j = p % N;
-				double s = 0;
-				for (int rr = 0; rr < 64; rr++) s += double(sx[rr][i]) * double(sw[rr][j]);
-				acc[q] += s;
+		for (int c = 0; c < 4; c++) acc[a][c] = 0;
+	if (active) {
+		const int64_t stride = int64_t(gridDim.x) * groups;
+		int64_t row = int64_t(blockIdx.x) * groups + grp;
+		for (; row + 3 * stride < n; row += 4 * stride) {
+			float4 a[4], c[4];
+#pragma unroll
+			for (int u = 0; u < 4; u++) {
+				a[u] = ld4_guard(X + (row + u * stride) * ldx, 4 * bi, M, vx);
+				c[u] = ld4_guard(W + (row + u * stride) * ldw, 4 * bj, N, vw);
+			}
+#pragma unroll
+			for (int u = 0; u < 4; u++) {
+				const double av[4] = {a[u].x, a[u].y, a[u].z, a[u].w}, cv[4] = {c[u].x, c[u].y, c[u].z, c[u].w};
+#pragma unroll
+				for (int p = 0; p < 4; p++)
+#pragma unroll
+					for (int q = 0; q < 4; q++) acc[p][q] = fma(av[p], cv[q], acc[p][q]);
 			}
 		}
-		__syncthreads();
-	}
+		for (; row < n; row += stride) {
+			const float4 a = ld4_guard(X + row * ldx, 4 * bi, M, vx);
+			const float4 c = ld4_guard(W + row * ldw, 4 * bj, N, vw);
+			const double av[4] = {a.x, a.y, a.z, a.w}, cv[4] = {c.x, c.y, c.z, c.w};
 #pragma unroll
-	for (int q = 0; q < 16; q++) {
-		const int p = tid + q * 256;
-		if (p < pairs) part[size_t(blockIdx.x) * pairs + p] = acc[q];
+			for (int p = 0; p < 4; p++)
+#pragma unroll
+				for (int q = 0; q < 4; q++) acc[p][q] = fma(av[p], cv[q], acc[p][q]);
+		}
+#pragma unroll
+		for (int p = 0; p < 4; p++)
+#pragma unroll
+			for (int q = 0; q < 4; q++) red[(size_t(grp) * nblk + blk) * 16 + p * 4 + q] = acc[p][q];
+	}
+	__syncthreads();
+	for (int pr = tid; pr < M * N; pr += 256) {
+		const int i = pr / N, j = pr % N;
+		const int b2 = (i / 4) * nbj + j / 4, e = (i % 4) * 4 + j % 4;
+		double sum = 0;
+		for (int g = 0; g < groups; g++) sum += red[(size_t(g) * nblk + b2) * 16 + e];
+		part[size_t(blockIdx.x) * M * N + pr] = sum;
 	}
 }
 

@@ -26,15 +26,18 @@
 // Precision modes:
 //   FMX_EIGEN_PLAIN  FP32 SpMM operands; every dense product on CUDA cores
 //                    with FP64 accumulation.
-//   FMX_EIGEN_MIXED  while the largest wanted residual exceeds `bf16_until`
-//                    (the low-precision phase): BF16 SpMM operands (FP32
-//                    accumulation), and the CholQR basis update and the
-//                    Rayleigh quotient Q^T W on tensor cores (3xTF32,
-//                    tcgen05); the CholQR Gram, the Cholesky factor, the
-//                    projected eigenproblem and the residual norms stay FP64.
-//                    After it, the passes are those of the plain mode (3xTF32
-//                    is accurate to about 1e-5 relative, too coarse for the
-//                    last digits of a 1e-6 residual).
+//   FMX_EIGEN_MIXED  the filter runs in correction form, Y = X p(Theta) + E,
+//                    with every filter SpMM on BF16 operands (FP32
+//                    accumulation): their rounding error is relative to the
+//                    correction E, which shrinks with the residual, so BF16
+//                    does not floor the accuracy.  The Rayleigh-Ritz SpMM
+//                    stays FP32.  While the largest wanted residual exceeds
+//                    `tensor_until`, the CholQR basis update and the Rayleigh
+//                    quotient Q^T W run on tensor cores (3xTF32, tcgen05),
+//                    after it in FP64 (3xTF32 is accurate to about 1e-5
+//                    relative).  The CholQR Gram, the Cholesky factor, the
+//                    projected eigenproblem and the residual norms are FP64
+//                    throughout.
 #include "fmx_internal.h"
 
 #include <cuda_runtime.h>
@@ -50,6 +53,7 @@ namespace eig {
 
 constexpr int kMaxB = 64;
 constexpr int kThreads = 256;
+constexpr int kMixedMaxDegree = 8;
 
 #define ECUDA_TRY(call)                                                         \
 	do {                                                                        \
@@ -99,70 +103,203 @@ __global__ void cheb_kernel(const float *__restrict__ W, const YT *__restrict__ 
 	}
 }
 
-// Basis update with FP64 accumulation, on row tiles of the n x b blocks:
+// One step of the filter in correction form, on flat n x b blocks:
+//   O = alpha W - ac0 E - beta P + cr[col] R + cx[col] X
+// (each of W, E, P, R, X may be absent)
+struct col_coefs {
+	float r[kMaxB];
+	float x[kMaxB];
+};
+
+__device__ __forceinline__ float4 ld4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
+__device__ __forceinline__ float4 ld4(const __nv_bfloat16 *p)
+{
+	const uint2 u = *reinterpret_cast<const uint2 *>(p);        // element 0 in the low half
+	return make_float4(__uint_as_float(u.x << 16), __uint_as_float(u.x & 0xffff0000u),
+			__uint_as_float(u.y << 16), __uint_as_float(u.y & 0xffff0000u));
+}
+__device__ __forceinline__ void st4(float *p, float4 v) { *reinterpret_cast<float4 *>(p) = v; }
+__device__ __forceinline__ void st4(__nv_bfloat16 *p, float4 v)
+{
+	__nv_bfloat162 a = __floats2bfloat162_rn(v.x, v.y), c = __floats2bfloat162_rn(v.z, v.w);
+	uint2 u;
+	u.x = *reinterpret_cast<uint32_t *>(&a);
+	u.y = *reinterpret_cast<uint32_t *>(&c);
+	*reinterpret_cast<uint2 *>(p) = u;
+}
+
+template <class ET, class PT, class OT>
+__global__ void corr_kernel(const float *__restrict__ W, const ET *__restrict__ E, const PT *__restrict__ P,
+		const float *__restrict__ R, const float *__restrict__ X, OT *__restrict__ O, int64_t count, int b,
+		float alpha, float ac0, float beta, col_coefs cf)
+{
+	const bool pow2 = (b & (b - 1)) == 0;
+	const int64_t tstride = int64_t(gridDim.x) * blockDim.x;
+	if ((b & 3) == 0) {
+		// four consecutive elements of one row per thread
+		for (int64_t i4 = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i4 < count / 4; i4 += tstride) {
+			const int64_t i = 4 * i4;
+			const int col = pow2 ? int(i & (b - 1)) : int(i % b);
+			float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+			if (W) {
+				const float4 t = ld4(W + i);
+				v = make_float4(alpha * t.x, alpha * t.y, alpha * t.z, alpha * t.w);
+			}
+			if (E) {
+				const float4 t = ld4(E + i);
+				v.x -= ac0 * t.x; v.y -= ac0 * t.y; v.z -= ac0 * t.z; v.w -= ac0 * t.w;
+			}
+			if (P) {
+				const float4 t = ld4(P + i);
+				v.x -= beta * t.x; v.y -= beta * t.y; v.z -= beta * t.z; v.w -= beta * t.w;
+			}
+			if (R) {
+				const float4 t = ld4(R + i);
+				v.x += cf.r[col] * t.x; v.y += cf.r[col + 1] * t.y; v.z += cf.r[col + 2] * t.z; v.w += cf.r[col + 3] * t.w;
+			}
+			if (X) {
+				const float4 t = ld4(X + i);
+				v.x += cf.x[col] * t.x; v.y += cf.x[col + 1] * t.y; v.z += cf.x[col + 2] * t.z; v.w += cf.x[col + 3] * t.w;
+			}
+			st4(O + i, v);
+		}
+		return;
+	}
+	for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < count; i += tstride) {
+		const int col = pow2 ? int(i & (b - 1)) : int(i % b);
+		float v = 0.f;
+		if (W) v = alpha * W[i];
+		if (E) v -= ac0 * ldf(E + i);
+		if (P) v -= beta * ldf(P + i);
+		if (R) v += cf.r[col] * R[i];
+		if (X) v += cf.x[col] * X[i];
+		stf(O + i, v);
+	}
+}
+
+// Basis update with FP64 accumulation:
 //   X[r][j] = sum_k Q[r][k] V[k][perm j]       (written when WRITE)
-//   NX[r][j] = sum_k W[r][k] V[k][perm j]      (HAS_W; written when WRITE)
+//   NX[r][j] = sum_k W[r][k] V[k][perm j]      (HAS_W; written when WRITE; with
+//                                               resid_out, NX - theta X instead)
 //   part[cta][j] += (NX[r][j] - theta[j] X[r][j])^2, part[cta][b + j] += X[r][j]^2   (RES)
-// Partials are summed in a fixed order (deterministic).
+// A thread owns one row and a group of up to 16 output columns (G = 1, 2 or
+// 4 threads per row for b <= 16, 32, 64); V sits in shared memory, read as a
+// broadcast.  Residual sums are reduced per warp with shuffles, then over the
+// warps in a fixed order (deterministic for a fixed grid).
+constexpr int kRitzCols = 16;
+
+__host__ __device__ inline int ritz_threads_per_row(int b) { return b <= 16 ? 1 : (b <= 32 ? 2 : 4); }
+
 template <bool HAS_W, bool RES, bool WRITE>
 __global__ void __launch_bounds__(kThreads)
 ritz_kernel(const float *__restrict__ Q, const float *__restrict__ W, int b, const double *__restrict__ V,
 		const int *__restrict__ perm, const double *__restrict__ theta, float *__restrict__ X,
-		float *__restrict__ NX, int64_t n, double *__restrict__ part)
+		float *__restrict__ NX, int64_t n, double *__restrict__ part, int resid_out)
 {
 	__shared__ double sV[kMaxB * kMaxB];
-	__shared__ float sQ[kThreads], sW[kThreads];
-	__shared__ double red[2 * kThreads];
+	__shared__ double red[kThreads / 32][2 * kMaxB];
 	const int tid = threadIdx.x;
-	const int R = kThreads / b;                  // rows per tile
-	for (int i = tid; i < b * b; i += kThreads) {
-		const int k = i / b, j = i % b;
-		sV[k * kMaxB + j] = V[k * b + (perm ? perm[j] : j)];
+	for (int i = tid; i < kMaxB * kMaxB; i += kThreads) {
+		const int k = i / kMaxB, j = i % kMaxB;
+		sV[i] = (k < b && j < b) ? V[k * b + (perm ? perm[j] : j)] : 0.0;
 	}
-	const int r = tid / b, j = tid % b;
-	const bool active = r < R;
-	const double th = (RES && active) ? theta[j] : 0.0;
-	double acc_r = 0, acc_x = 0;
-	for (int64_t r0 = int64_t(blockIdx.x) * R; r0 < n; r0 += int64_t(gridDim.x) * R) {
-		__syncthreads();
-		const int64_t base = r0 * b;
-		const int64_t lim = min(int64_t(R), n - r0) * b;
-		if (tid < lim) {
-			sQ[tid] = Q[base + tid];
-			if (HAS_W) sW[tid] = W[base + tid];
-		}
-		__syncthreads();
-		if (active && r0 + r < n) {
-			double x = 0, y = 0;
+	__syncthreads();
+	const int G = ritz_threads_per_row(b);
+	const int g = tid % G;
+	const int j0 = g * kRitzCols;
+	double th[kRitzCols];
+#pragma unroll
+	for (int jj = 0; jj < kRitzCols; jj++) th[jj] = (RES && j0 + jj < b) ? theta[j0 + jj] : 0.0;
+	double racc[kRitzCols], xacc[kRitzCols];
+#pragma unroll
+	for (int jj = 0; jj < kRitzCols; jj++) racc[jj] = xacc[jj] = 0;
+	const int64_t rows_per_pass = int64_t(gridDim.x) * (kThreads / G);
+	const bool vec = (b % 4) == 0;
+	for (int64_t row = int64_t(blockIdx.x) * (kThreads / G) + tid / G; row < n; row += rows_per_pass) {
+		const float *q = Q + row * b;
+		const float *w = HAS_W ? W + row * b : nullptr;
+		double x[kRitzCols], y[kRitzCols];
+#pragma unroll
+		for (int jj = 0; jj < kRitzCols; jj++) x[jj] = y[jj] = 0;
+		if (vec) {
+			// chunks of 16 input columns: all loads first (8 x 16 bytes in
+			// flight), then the FMAs
+			for (int k0 = 0; k0 < b; k0 += 16) {
+				const int kn = min(16, b - k0);             // a multiple of 4
+				float qs[16], ws[16];
+#pragma unroll
+				for (int u = 0; u < 4; u++) {
+					float4 qv = make_float4(0.f, 0.f, 0.f, 0.f), wv = qv;
+					if (4 * u < kn) {
+						qv = *reinterpret_cast<const float4 *>(q + k0 + 4 * u);
+						if (HAS_W) wv = *reinterpret_cast<const float4 *>(w + k0 + 4 * u);
+					}
+					qs[4 * u] = qv.x; qs[4 * u + 1] = qv.y; qs[4 * u + 2] = qv.z; qs[4 * u + 3] = qv.w;
+					ws[4 * u] = wv.x; ws[4 * u + 1] = wv.y; ws[4 * u + 2] = wv.z; ws[4 * u + 3] = wv.w;
+				}
+#pragma unroll
+				for (int u = 0; u < 16; u++) {
+					const double *vr = sV + (k0 + u) * kMaxB + j0;   // rows >= b of sV are zero
+#pragma unroll
+					for (int jj = 0; jj < kRitzCols; jj++) {
+						x[jj] = fma(double(qs[u]), vr[jj], x[jj]);
+						if (HAS_W) y[jj] = fma(double(ws[u]), vr[jj], y[jj]);
+					}
+				}
+			}
+		} else {
 			for (int k = 0; k < b; k++) {
-				const double v = sV[k * kMaxB + j];
-				x += double(sQ[r * b + k]) * v;
-				if (HAS_W) y += double(sW[r * b + k]) * v;
+				const double qk = q[k];
+				const double wk = HAS_W ? double(w[k]) : 0.0;
+				const double *vr = sV + k * kMaxB + j0;
+#pragma unroll
+				for (int jj = 0; jj < kRitzCols; jj++) {
+					x[jj] = fma(qk, vr[jj], x[jj]);
+					if (HAS_W) y[jj] = fma(wk, vr[jj], y[jj]);
+				}
 			}
-			if (WRITE) {
-				X[base + tid] = float(x);
-				if (HAS_W) NX[base + tid] = float(y);
-			}
-			if (RES) {
-				const double d = y - th * x;
-				acc_r += d * d;
-				acc_x += x * x;
+		}
+		if (WRITE) {
+			float *xo = X + row * b + j0;
+			float *yo = HAS_W ? NX + row * b + j0 : nullptr;
+#pragma unroll
+			for (int jj = 0; jj < kRitzCols; jj++)
+				if (j0 + jj < b) {
+					xo[jj] = float(x[jj]);
+					if (HAS_W) yo[jj] = float(resid_out ? y[jj] - th[jj] * x[jj] : y[jj]);
+				}
+		}
+		if (RES) {
+#pragma unroll
+			for (int jj = 0; jj < kRitzCols; jj++) {
+				const double d = y[jj] - th[jj] * x[jj];
+				racc[jj] = fma(d, d, racc[jj]);
+				xacc[jj] = fma(x[jj], x[jj], xacc[jj]);
 			}
 		}
 	}
 	if (RES) {
-		__syncthreads();
-		red[tid] = acc_r;
-		red[kThreads + tid] = acc_x;
-		__syncthreads();
-		if (tid < b) {
-			double sr = 0, sx = 0;
-			for (int q = 0; q < R; q++) {
-				sr += red[q * b + tid];
-				sx += red[kThreads + q * b + tid];
+		const int lane = tid & 31, warp = tid >> 5;
+#pragma unroll
+		for (int jj = 0; jj < kRitzCols; jj++) {
+			for (int off = 16; off >= G; off >>= 1) {
+				racc[jj] += __shfl_down_sync(0xffffffffu, racc[jj], off);
+				xacc[jj] += __shfl_down_sync(0xffffffffu, xacc[jj], off);
 			}
-			part[size_t(blockIdx.x) * 2 * b + tid] = sr;
-			part[size_t(blockIdx.x) * 2 * b + b + tid] = sx;
+		}
+		if (lane < G) {
+#pragma unroll
+			for (int jj = 0; jj < kRitzCols; jj++)
+				if (j0 + jj < b) {
+					red[warp][j0 + jj] = racc[jj];
+					red[warp][b + j0 + jj] = xacc[jj];
+				}
+		}
+		__syncthreads();
+		for (int i = tid; i < 2 * b; i += kThreads) {
+			double sum = 0;
+			for (int w2 = 0; w2 < kThreads / 32; w2++) sum += red[w2][i];
+			part[size_t(blockIdx.x) * 2 * b + i] = sum;
 		}
 	}
 }
@@ -321,8 +458,8 @@ struct solver {
 		E_TRY(ws.get(&tc_err, 1));
 		E_TRY(ws.get(&info, 4));
 		E_TRY(ws.get(&dsmall, 1));
-		const int R = kThreads / b;
-		ritz_grid = int(std::max<int64_t>(1, std::min<int64_t>((n + R - 1) / R, int64_t(sm_count()) * 4)));
+		const int R = kThreads / ritz_threads_per_row(b);     // rows per CTA and pass
+		ritz_grid = int(std::max<int64_t>(1, std::min<int64_t>((n + R - 1) / R, int64_t(sm_count()) * 2)));
 		E_TRY(ws.get(&part, size_t(ritz_grid) * 2 * b));
 		const int gparts = std::max({fmx_dense_gram_parts(FMX_DENSE_F64, n), fmx_dense_gram_parts(FMX_DENSE_TF32X3, n)});
 		E_TRY(ws.get(&gpart, size_t(gparts) * b * b * 2));      // room for double partials
@@ -348,6 +485,9 @@ struct solver {
 	// residuals there)
 	bool lowp = false;
 	bool tensor_cores() const { return lowp; }
+	// mixed precision: the filter runs in correction form on BF16 operands and
+	// the Rayleigh-Ritz step leaves R = A_s X - X Theta in NX
+	bool corr = false;
 
 	// Y (n x b) -> orthonormal Q (n x b) by two passes of CholQR; the first
 	// is shifted.  `pass` selects the chol info slot pair (0 or 2).
@@ -368,7 +508,7 @@ struct solver {
 				E_TRY(fmx_dense_gemm(FMX_DENSE_TF32X3, in, b, n, b, Tf, b, b, outs[p], b, tc_err, st));
 			} else {
 				ritz_kernel<false, false, true><<<ritz_grid, kThreads, 0, st>>>(in, nullptr, b, T, nullptr, nullptr,
-						outs[p], nullptr, n, nullptr);
+						outs[p], nullptr, n, nullptr, 0);
 				ECUDA_TRY(cudaGetLastError());
 			}
 			in = outs[p];
@@ -391,7 +531,8 @@ struct solver {
 		E_TRY(fmx_dense_sym_eig(H, b, wv, V, st));
 		order_kernel<<<1, 1, 0, st>>>(wv, b, o.which == FMX_EIGEN_LM, perm, dsmall->theta);
 		ECUDA_TRY(cudaGetLastError());
-		ritz_kernel<true, true, true><<<ritz_grid, kThreads, 0, st>>>(Q, W, b, V, perm, dsmall->theta, X, NX, n, part);
+		ritz_kernel<true, true, true><<<ritz_grid, kThreads, 0, st>>>(Q, W, b, V, perm, dsmall->theta, X, NX, n, part,
+				int(corr));
 		ECUDA_TRY(cudaGetLastError());
 		return finish_small();
 	}
@@ -429,7 +570,7 @@ struct solver {
 	{
 		E_TRY(spmm(FMX_F32, X, b, W));
 		ritz_kernel<true, true, false><<<ritz_grid, kThreads, 0, st>>>(X, W, b, eye, nullptr, dsmall->theta, nullptr,
-				nullptr, n, part);
+				nullptr, n, part, 0);
 		ECUDA_TRY(cudaGetLastError());
 		return finish_small();
 	}
@@ -443,43 +584,23 @@ struct solver {
 		return FMX_OK;
 	}
 
-	// Y_m = p_m(A_s) X into B[k]; returns k.  Y_1 comes from NX = A_s X.
-	int filter(double cut, bool lowp, int *out_k)
+	// Y_m = p_m(A_s) X into B[k] (FP32); returns k.  Y_1 comes from NX = A_s X.
+	int filter(double cut, int mdeg, int *out_k)
 	{
-		const int mdeg = o.degree;
 		double lo = o.lower, up = o.upper;
 		if (o.which == FMX_EIGEN_LM) lo = -cut;
 		const double e = std::max((cut - lo) / 2, 1e-12 * (up - lo));
 		const double c0 = (cut + lo) / 2;
 		const double s1 = e / (up - c0);
 		double sj = s1;
-		typedef __nv_bfloat16 bf;
-		// Y1 (index 0 in B)
-		int cur = 0;
-		const bool last1 = mdeg == 1;
-		if (lowp && !last1) E_TRY(cheb(NX, X, (const float *)nullptr, (bf *)B[0], float(s1 / e), float(c0), 0.f));
-		else E_TRY(cheb(NX, X, (const float *)nullptr, B[0], float(s1 / e), float(c0), 0.f));
-		int prev = -1;                                    // -1 = X
+		E_TRY(cheb(NX, X, (const float *)nullptr, B[0], float(s1 / e), float(c0), 0.f));
+		int cur = 0, prev = -1;                           // prev -1 = X
 		for (int j = 2; j <= mdeg; j++) {
 			const double sn = 1.0 / (2.0 / s1 - sj);
-			const float alpha = float(2 * sn / e), beta = float(sj * sn);
-			const bool cur_bf = lowp;                     // Y_{j-1} is BF16 when lowp (j - 1 < m)
-			const bool prev_bf = lowp && prev >= 0;
-			const bool out_bf = lowp && j < mdeg;
-			E_TRY(spmm(cur_bf ? FMX_BF16 : FMX_F32, B[cur], b, W));
+			E_TRY(spmm(FMX_F32, B[cur], b, W));
 			const int nxt = (cur + 1) % 3 == prev ? (cur + 2) % 3 : (cur + 1) % 3;
-			const void *P = prev < 0 ? static_cast<const void *>(X) : static_cast<const void *>(B[prev]);
-			int rc;
-			if (cur_bf) {
-				const bf *Y = (const bf *)B[cur];
-				if (prev_bf) rc = out_bf ? cheb(W, Y, (const bf *)P, (bf *)B[nxt], alpha, float(c0), beta)
-				                         : cheb(W, Y, (const bf *)P, B[nxt], alpha, float(c0), beta);
-				else rc = out_bf ? cheb(W, Y, (const float *)P, (bf *)B[nxt], alpha, float(c0), beta)
-				                 : cheb(W, Y, (const float *)P, B[nxt], alpha, float(c0), beta);
-			} else {
-				rc = cheb(W, (const float *)B[cur], (const float *)P, B[nxt], alpha, float(c0), beta);
-			}
-			E_TRY(rc);
+			const float *P = prev < 0 ? X : B[prev];
+			E_TRY(cheb(W, (const float *)B[cur], P, B[nxt], float(2 * sn / e), float(c0), float(sj * sn)));
 			prev = cur;
 			cur = nxt;
 			sj = sn;
@@ -488,11 +609,113 @@ struct solver {
 		return FMX_OK;
 	}
 
+	template <class ET, class PT, class OT>
+	int corr_step(const float *Wm, const ET *E, const PT *P, const float *R, const float *Xs, OT *Out, float alpha,
+			float ac0, float beta, const col_coefs &cf)
+	{
+		const int64_t cnt = n * b;
+		corr_kernel<ET, PT, OT><<<flat_grid(cnt), kThreads, 0, st>>>(Wm, E, P, R, Xs, Out, cnt, b, alpha, ac0, beta, cf);
+		ECUDA_TRY(cudaGetLastError());
+		return FMX_OK;
+	}
+
+	// The same filter in correction form: Y_j = X D_j + E_j with D_j =
+	// p_j(Theta) (diagonal, carried on the host) and
+	//   E_1 = a_1 R,   E_j = a_j (A_s E_{j-1} - c0 E_{j-1} + R D_{j-1}) - b_j E_{j-2},
+	// where R = A_s X - X Theta comes from the last Rayleigh-Ritz step.  The
+	// SpMMs act on E_j in BF16: their rounding error is relative to the
+	// correction, which shrinks with the residual, so BF16 operands do not
+	// floor the attainable accuracy.  Y_m = X D_m + E_m is written in FP32.
+	int filter_corr(double cut, int mdeg, int *out_k)
+	{
+		double lo = o.lower, up = o.upper;
+		if (o.which == FMX_EIGEN_LM) lo = -cut;
+		const double e = std::max((cut - lo) / 2, 1e-12 * (up - lo));
+		const double c0 = (cut + lo) / 2;
+		const double s1 = e / (up - c0);
+		typedef __nv_bfloat16 bf;
+		const float *R = NX;
+		std::vector<double> Dp(b, 1.0), Dc(b), Dn(b);     // D_{j-2}, D_{j-1}, D_j
+		for (int j = 0; j < b; j++) Dc[j] = (s1 / e) * (hsmall->theta[j] - c0);
+		col_coefs cf{};
+		// E_1 (or Y_1 when m = 1)
+		for (int j = 0; j < b; j++) {
+			cf.r[j] = float(s1 / e);
+			cf.x[j] = float(Dc[j]);
+		}
+		if (mdeg == 1) {
+			E_TRY(corr_step((const float *)nullptr, (const float *)nullptr, (const float *)nullptr, R, X, B[0], 0.f,
+					0.f, 0.f, cf));
+			*out_k = 0;
+			return FMX_OK;
+		}
+		E_TRY(corr_step((const float *)nullptr, (const float *)nullptr, (const float *)nullptr, R,
+				(const float *)nullptr, (bf *)B[0], 0.f, 0.f, 0.f, cf));
+		int cur = 0, prev = -1;
+		double sj = s1;
+		for (int jdeg = 2; jdeg <= mdeg; jdeg++) {
+			const double sn = 1.0 / (2.0 / s1 - sj);
+			const double alpha = 2 * sn / e, beta = sj * sn;
+			const bool last = jdeg == mdeg;
+			E_TRY(spmm(FMX_BF16, B[cur], b, W));
+			for (int j = 0; j < b; j++) {
+				Dn[j] = alpha * (hsmall->theta[j] - c0) * Dc[j] - beta * Dp[j];
+				cf.r[j] = float(alpha * Dc[j]);
+				cf.x[j] = float(Dn[j]);
+			}
+			const int nxt = (cur + 1) % 3 == prev ? (cur + 2) % 3 : (cur + 1) % 3;
+			const bf *E = (const bf *)B[cur];
+			const bf *P = prev < 0 ? nullptr : (const bf *)B[prev];
+			const float a = float(alpha), ac = float(alpha * c0), bt = float(beta);
+			if (last) E_TRY(corr_step(W, E, P, R, X, B[nxt], a, ac, bt, cf));
+			else E_TRY(corr_step(W, E, P, R, (const float *)nullptr, (bf *)B[nxt], a, ac, bt, cf));
+			prev = cur;
+			cur = nxt;
+			sj = sn;
+			Dp.swap(Dc);
+			Dc.swap(Dn);
+		}
+		*out_k = cur;
+		return FMX_OK;
+	}
+
+	// Filter degree for the next pass (the per-vector degree rule of ChASE,
+	// Winkelmann et al., ACM TOMS 45(2), 2019, applied to the slowest wanted
+	// vector): a Ritz pair at theta_j, with the damped interval [lo, cut]
+	// mapped to [-1, 1], has its residual divided by about T_m(t_j), t_j =
+	// (theta_j - c0) / e, after m steps.  So m = acosh(r_j / tol) / acosh(t_j),
+	// rounded up, at least 2 and at most o.degree; o.degree when a wanted
+	// Ritz value lies inside the damped interval.
+	int degree_for(double cut) const
+	{
+		double lo = o.lower;
+		if (o.which == FMX_EIGEN_LM) lo = -cut;
+		const double e = std::max((cut - lo) / 2, 1e-12 * (o.upper - o.lower));
+		const double c0 = (cut + lo) / 2;
+		const double target = 0.5 * o.tol;
+		double m = 2;
+		for (int j = 0; j < o.nev; j++) {
+			const double r = residual(j);
+			if (r <= target) continue;
+			const double th = o.which == FMX_EIGEN_LM ? std::fabs(hsmall->theta[j]) : hsmall->theta[j];
+			const double t = (th - c0) / e;
+			if (!(t > 1.0 + 1e-9)) return max_degree();
+			m = std::max(m, std::ceil(std::acosh(r / target) / std::acosh(t)));
+		}
+		return int(std::min<double>(m, max_degree()));
+	}
+
+	// In correction form the BF16 error of the recurrence grows with its
+	// length; measured on R-MAT scale 22 (top 8), caps above 8 cost the mixed
+	// mode more passes than they save, so it filters with at most 8 steps.
+	int max_degree() const { return corr ? std::min(o.degree, kMixedMaxDegree) : o.degree; }
+
 	int run(double *evals, float *evecs, int64_t ldv, double *residuals, fmx_eigen_status *status)
 	{
 		const auto t0 = std::chrono::steady_clock::now();
 		E_TRY(setup());
 		lowp = o.precision == FMX_EIGEN_MIXED;
+		corr = o.precision == FMX_EIGEN_MIXED;
 		// start block
 		if (o.X0) {
 			ECUDA_TRY(cudaMemcpy2DAsync(B[0], size_t(b) * sizeof(float), o.X0, size_t(o.ldx0) * sizeof(float),
@@ -524,9 +747,11 @@ struct solver {
 			cut = std::min(cut, cap);
 			if (o.which == FMX_EIGEN_LA) cut = std::max(cut, o.lower + 1e-6 * (o.upper - o.lower));
 			else cut = std::max(cut, 1e-6 * o.upper);
-			lowp = o.precision == FMX_EIGEN_MIXED && maxres > o.bf16_until;
+			lowp = o.precision == FMX_EIGEN_MIXED && maxres > o.tensor_until;
 			int k = 0;
-			E_TRY(filter(cut, lowp, &k));
+			const int mdeg = degree_for(cut);
+			if (corr) E_TRY(filter_corr(cut, mdeg, &k));
+			else E_TRY(filter(cut, mdeg, &k));
 			E_TRY(cholqr2(B[k], B[(k + 1) % 3], B[(k + 2) % 3]));
 			E_TRY(rayleigh_ritz(B[(k + 2) % 3]));
 			maxres = max_residual(o.nev);
@@ -574,14 +799,14 @@ void fmx_eigen_default_options(fmx_eigen_options *o, int nev)
 	std::memset(o, 0, sizeof(*o));
 	o->nev = nev;
 	o->block_size = std::min(kMaxB, std::max(2 * nev, 16));
-	o->degree = 10;
+	o->degree = 16;
 	o->max_iters = 500;
 	o->which = FMX_EIGEN_LA;
 	o->precision = FMX_EIGEN_PLAIN;
 	o->tol = 1e-8;
 	o->lower = -1.0;
 	o->upper = 1.0;
-	o->bf16_until = 1e-2;
+	o->tensor_until = 1e-3;
 	o->seed = 1;
 	o->X0 = nullptr;
 	o->ldx0 = 0;

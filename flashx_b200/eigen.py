@@ -23,8 +23,9 @@ class eigen_options:
     """eigen_options (eigensolver.h:57-73): same field names and defaults
     (tol 1e-8, max_iters 500, which "LM").  The reference picks an Anasazi
     solver by name; here every name runs the same block Chebyshev iteration,
-    with block_size >= nev.  Extra fields: degree (SpMMs per filter pass),
-    precision ("plain" or "mixed"), bf16_until, lower/upper (spectrum bounds;
+    with block_size >= nev.  Extra fields: degree (the largest number of SpMMs
+    per filter pass; each pass picks what its slowest residual needs),
+    precision ("plain" or "mixed"), tensor_until, lower/upper (spectrum bounds;
     [-1, 1] holds for D^-1/2 A D^-1/2), seed."""
 
     def __init__(self):
@@ -37,9 +38,9 @@ class eigen_options:
         self.solver = "KrylovSchur"
         self.which = "LM"
         self.in_mem = True
-        self.degree = 10
+        self.degree = 16
         self.precision = "plain"
-        self.bf16_until = 1e-2
+        self.tensor_until = 1e-3
         self.lower = -1.0
         self.upper = 1.0
         self.seed = 1
@@ -69,7 +70,7 @@ class eigen_options:
         o.tol = float(self.tol)
         o.lower = float(self.lower)
         o.upper = float(self.upper)
-        o.bf16_until = float(self.bf16_until)
+        o.tensor_until = float(self.tensor_until)
         o.seed = int(self.seed)
         return o
 

@@ -228,15 +228,17 @@ int fmx_dense_sym_eig(const double *H, int b, double *w, double *V, void *stream
 #define FMX_EIGEN_LA 0      /* largest algebraic ("LA") */
 #define FMX_EIGEN_LM 1      /* largest magnitude ("LM", the reference's default) */
 #define FMX_EIGEN_PLAIN 0   /* FP32 SpMM operands; dense products in FP64 on CUDA cores */
-#define FMX_EIGEN_MIXED 1   /* BF16 SpMM operands until bf16_until, then FP32; CholQR
-                               basis update and Rayleigh quotient on tensor cores
-                               (3xTF32); CholQR Gram, Cholesky, projected problem
-                               and residual norms in FP64 */
+#define FMX_EIGEN_MIXED 1   /* filter in correction form with BF16 SpMM operands (FP32
+                               accumulation), Rayleigh-Ritz SpMM in FP32; CholQR basis
+                               update and Rayleigh quotient on tensor cores (3xTF32)
+                               until tensor_until, FP64 after; CholQR Gram, Cholesky,
+                               projected problem and residual norms in FP64 */
 
 typedef struct fmx_eigen_options {
 	int nev;            /* wanted eigenpairs (eigen_options::nev) */
 	int block_size;     /* vectors per block, nev <= block_size <= 64 */
-	int degree;         /* Chebyshev degree per filter pass (SpMMs per pass) */
+	int degree;         /* largest Chebyshev degree of a filter pass (SpMMs per pass);
+	                       each pass picks the degree its slowest wanted residual needs */
 	int max_iters;      /* filter passes (eigen_options::max_iters) */
 	int which;          /* FMX_EIGEN_LA or FMX_EIGEN_LM (eigen_options::which) */
 	int precision;      /* FMX_EIGEN_PLAIN or FMX_EIGEN_MIXED */
@@ -244,8 +246,8 @@ typedef struct fmx_eigen_options {
 	double lower;       /* lower bound of the spectrum (-1 for D^-1/2 A D^-1/2) */
 	double upper;       /* upper bound of the spectrum (1 for D^-1/2 A D^-1/2); ||A|| is
 	                       taken as max(|lower|, |upper|) */
-	double bf16_until;  /* FMX_EIGEN_MIXED: BF16 filter while the largest residual
-	                       exceeds this */
+	double tensor_until;/* FMX_EIGEN_MIXED: dense products on tensor cores while the
+	                       largest residual exceeds this */
 	uint64_t seed;      /* random start block, uniform(-1, 1) (MvRandom) */
 	const float *X0;    /* optional start block on the device (n x block_size), or NULL */
 	int64_t ldx0;
@@ -261,7 +263,7 @@ typedef struct fmx_eigen_status {
 } fmx_eigen_status;
 
 /* Defaults as eigen_options() and init(nev) (eigensolver.cpp:82-116): tol 1e-8,
- * max_iters 500, block_size max(2 nev, 16) (at most 64), degree 10, LA, plain,
+ * max_iters 500, block_size max(2 nev, 16) (at most 64), degree 16, LA, plain,
  * spectrum [-1, 1], seed 1. */
 void fmx_eigen_default_options(fmx_eigen_options *opts, int nev);
 
@@ -278,6 +280,44 @@ int fmx_eigen_solve(const fmx_matrix *m, const float *row_scale,
  * NA_eigen_Operator (matrix/test/test-eigen.cpp:96-109); s is a device array
  * of n floats. */
 int fmx_na_scale(const fmx_matrix *m, float *s, void *stream);
+
+/* ---- learned warm start ---------------------------------------------------------
+ * A 2-layer graph network that maps vertex features to a start block for
+ * fmx_eigen_solve (no counterpart in the reference):
+ *   F  (n x 16)  standardised log(1 + degree), then 15 N(0,1) channels (seeded)
+ *   Z  (n x 64)  [F, A_s F, A_s^2 F, A_s^3 F]    (A_s = diag(s) A diag(s))
+ *   H  (n x 64)  relu(Z W1 + b1)
+ *   Y  (n x 16)  A_s (H W2)
+ * trained to align span(Y) with given eigenvectors U (loss 1 - ||U^T Q||_F^2 /
+ * nev, Q an orthonormal basis of span(Y)).  Weights are FP32 master copies
+ * (Adam) that enter every product as BF16 (FMX_DENSE_BF16: tcgen05, FP32
+ * accumulation) or split 3xTF32 (FMX_DENSE_TF32X3, for gradient checks).
+ * Parameters, flat: W1 (64 x 64, row-major), b1 (64), W2 (64 x 16). */
+#define FMX_GNN_FEATURES 64
+#define FMX_GNN_OUT 16
+#define FMX_GNN_PARAMS 5184
+
+typedef struct fmx_gnn fmx_gnn;
+/* Glorot-uniform weights from `seed`, zero bias, zero optimiser state. */
+int fmx_gnn_create(int device, uint64_t seed, fmx_gnn **out);
+int fmx_gnn_free(fmx_gnn *g);
+/* Copy FMX_GNN_PARAMS floats in (resets the optimiser state) or out. */
+int fmx_gnn_set_params(fmx_gnn *g, const float *host);
+int fmx_gnn_get_params(const fmx_gnn *g, float *host);
+/* Z (n x 64 device floats) for matrix m with row scale s (NULL: none). */
+int fmx_gnn_features(const fmx_matrix *m, const float *row_scale, uint64_t seed,
+                     float *Z, void *stream);
+/* Y (n x 16 device floats). */
+int fmx_gnn_forward(const fmx_gnn *g, const fmx_matrix *m, const float *row_scale,
+                    const float *Z, int precision, float *Y, void *stream);
+/* Forward, loss against U (n x nev device floats, ldu), backward into the
+ * model's gradient buffer; *loss (host) and grad_host (FMX_GNN_PARAMS floats)
+ * are optional.  Synchronises the stream. */
+int fmx_gnn_loss_grad(fmx_gnn *g, const fmx_matrix *m, const float *row_scale,
+                      const float *Z, const float *U, int64_t ldu, int nev,
+                      int precision, double *loss, float *grad_host, void *stream);
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8) with the stored gradient. */
+int fmx_gnn_adam_step(fmx_gnn *g, float lr, void *stream);
 
 /* ---- synthetic graphs ---------------------------------------------------------
  * R-MAT edges (a,b,c; d = 1-a-b-c) of 2^scale vertices, counter-based so the
