@@ -13,6 +13,14 @@ column indices ~1 GB) are larger than the 126 MB L2, so no flush is needed.
   python bench.py [--gpus N --steps K --warmup W] [--impl fmx|reference]
       [--scale 24 --k 16 --weighted]
 
+The line's "eigen" object (rank 0, after the SpMM timing; --skip-eigen
+leaves it out) times the block eigensolver on its configuration: top 8
+eigenpairs of D^-1/2 A D^-1/2 of the symmetrised R-MAT scale 22 graph, block
+16, residual 1e-6, plain against mixed precision and against mixed precision
+started from the learned warm start (weights in
+flashx_b200/warmstart_weights.f32), plus that comparison on held-out SBM
+graphs.
+
 --impl reference times the reference's CPU SpMM algorithm (the oracle's C
 restatement of FlashMatrix's 2D traversal; the reference library itself
 cannot be built here) on all host cores over a bounded sample of block rows.
@@ -48,6 +56,9 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample time")
     p.add_argument("--e2e-steps", type=int, default=5)
     p.add_argument("--skip-cpu", action="store_true")
+    p.add_argument("--skip-eigen", action="store_true")
+    p.add_argument("--eig-scale", type=int, default=22, help="R-MAT scale of the eigensolver workload")
+    p.add_argument("--eig-sbm", type=int, default=20, help="held-out SBM graphs for the learned warm start")
     return p.parse_args()
 
 
@@ -195,6 +206,89 @@ def read_traffic(name):
         return None
 
 
+def _timed_solve(torch, dev, fn, reps=3):
+    """Median wall time (ms, CUDA events on the current stream) of `fn`,
+    after one untimed call; returns (ms, last result)."""
+    fn()
+    times, res = [], None
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        res = fn()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        times.append(e0.elapsed_time(e1))
+    return float(np.median(times)), res
+
+
+def _solve_summary(ms, r):
+    return {"ms": round(ms, 2), "spmm_calls": int(r.status.spmm_calls), "num_ops": int(r.status.num_ops),
+            "iters": int(r.status.num_iters), "converged": int(r.status.converged),
+            "max_residual": float(r.status.max_residual)}
+
+
+def eigen_measure(a, dev):
+    """The eigensolver configuration: top 8 eigenpairs of D^-1/2 A D^-1/2 of
+    a symmetrised R-MAT graph (scale a.eig_scale, edge factor 16, seed 1),
+    block 16, residual 1e-6: plain (FP32 SpMM, FP64 dense) against mixed
+    (BF16 correction-form filter, tensor-core dense early), each with a random
+    start and the mixed one also with the learned start; then the learned
+    start against the random one on held-out SBM graphs (committed weights)."""
+    import torch
+    from flashx_b200 import matrix_image, sparse_matrix
+    from flashx_b200.eigen import NA_operator, compute_eigen
+    from flashx_b200.graphs import rmat_edges, symmetrize
+    from flashx_b200 import warmstart as ws
+    n = 1 << a.eig_scale
+    t0 = time.time()
+    s, d = rmat_edges(a.eig_scale, seed=1)
+    s, d = symmetrize(s, d)
+    m = sparse_matrix.create(matrix_image.build(s, d, None, nrows=n, ncols=n, block_size=(16384, 16384),
+                                                dedup=True), None, device=dev.index)
+    del s, d
+    op = NA_operator(m, device=dev.index)
+    out = {"workload": f"rmat-s{a.eig_scale}-ef16-symmetrised-na-top8-block16-tol1e-6", "n": n,
+           "nnz": int(m.get_nnz()), "build_s": round(time.time() - t0, 2),
+           "timing": "median of 3 after 1 warm-up, CUDA events around the whole solve (host loop included)"}
+    for prec in ("plain", "mixed"):
+        o = ws.eigen_opts(8, 1e-6, prec)
+        ms, r = _timed_solve(torch, dev, lambda: compute_eigen(op, True, o))
+        out[prec] = _solve_summary(ms, r)
+    out["speedup_mixed_vs_plain"] = round(out["plain"]["ms"] / out["mixed"]["ms"], 3)
+    weights = os.path.join(ROOT, "flashx_b200", "warmstart_weights.f32")
+    if not os.path.exists(weights):
+        out["learned"] = "no committed weights"
+        return out
+    net = ws.warm_start_net.load(weights, dev.index)
+    o = ws.eigen_opts(8, 1e-6, "mixed")
+    ms, r = _timed_solve(torch, dev, lambda: compute_eigen(op, True, o, X0=net.start_block(op)))
+    out["mixed_learned"] = _solve_summary(ms, r)
+    out["mixed_learned"]["spmm_calls"] += ws.SPMM_PER_START
+    out["speedup_learned_mixed_vs_plain"] = round(out["plain"]["ms"] / ms, 3)
+    del op, m
+    rows = []
+    for i in range(a.eig_sbm):
+        inst = ws.sbm_instance(30_000_000 + i, solve=False)
+        po, mo = ws.eigen_opts(inst.nev, 1e-6, "plain"), ws.eigen_opts(inst.nev, 1e-6, "mixed")
+        ms_p, rp = _timed_solve(torch, dev, lambda: compute_eigen(inst.op, True, po), reps=1)
+        ms_w, rw = _timed_solve(torch, dev, lambda: compute_eigen(inst.op, True, mo,
+                                                                  X0=net.start_block(inst.op, 0, mo.block_size)),
+                                reps=1)
+        rows.append((ms_p, int(rp.status.spmm_calls), ms_w, int(rw.status.spmm_calls) + ws.SPMM_PER_START,
+                     int(rp.status.converged == inst.nev and rw.status.converged == inst.nev)))
+        del inst
+    R = np.array(rows)
+    out["sbm_heldout"] = {
+        "graphs": a.eig_sbm, "n": "uniform 10k-200k", "blocks": "4-16 (nev = blocks)", "ratio": "5-20",
+        "plain_random_ms_median": round(float(np.median(R[:, 0])), 2),
+        "mixed_learned_ms_median": round(float(np.median(R[:, 2])), 2),
+        "plain_random_spmm_sum": int(R[:, 1].sum()), "mixed_learned_spmm_sum": int(R[:, 3].sum()),
+        "speedup_total_time": round(float(R[:, 0].sum() / R[:, 2].sum()), 3), "all_converged": int(R[:, 4].sum())}
+    return out
+
+
 def run_reference(a, rank, world):
     if rank != 0:
         return
@@ -331,6 +425,12 @@ def main():
         cpu = {"value": round(gbs[0], 3), "unit": "GB/s", "cores": nthreads, "kind": "port",
                "sample": sample + f"; CPU: {model}"}
 
+    eig = None
+    if rank == 0 and not a.skip_eigen:
+        del m, X, Y
+        torch.cuda.empty_cache()
+        eig = eigen_measure(a, dev)
+
     if rank == 0:
         line = {
             "metric": "SpMM GB/s (algorithmic bytes / time)",
@@ -355,6 +455,7 @@ def main():
             "e2e": e2e,
             "gpu_launches": a.steps * kernels,
             "clocks": clk,
+            "eigen": eig,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

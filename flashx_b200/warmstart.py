@@ -81,9 +81,18 @@ class warm_start_net:
                                   Y.data_ptr(), st))
         return Y
 
-    def start_block(self, op, seed=0):
-        """The warm start X0 (n x 16) for compute_eigen (4 SpMMs)."""
-        return self.forward(op, self.features(op, seed))
+    def start_block(self, op, seed=0, block_size=_lib.GNN_OUT):
+        """The warm start X0 (n x block_size) for compute_eigen (4 SpMMs):
+        the network's 16 columns, then uniform(-1, 1) columns if the block is
+        wider."""
+        import torch
+        Y = self.forward(op, self.features(op, seed))
+        if block_size <= _lib.GNN_OUT:
+            return Y[:, :block_size].contiguous()
+        g = torch.Generator(device=Y.device)
+        g.manual_seed(seed)
+        extra = torch.rand((Y.shape[0], block_size - _lib.GNN_OUT), generator=g, device=Y.device) * 2 - 1
+        return torch.cat([Y, extra], 1).contiguous()
 
     def loss_grad(self, op, Z, U, precision="bf16", want_grad=False, stream=None):
         import torch
@@ -139,10 +148,18 @@ class sbm_instance:
             self.solve_status = res.status
 
 
+def block_size_for(nev):
+    """16 columns (the network's output) while they leave guard vectors
+    (nev <= 8); else nev + 8 rounded up to a multiple of 8, the extra columns
+    of a learned start being random.  With block_size == nev the filter's cut
+    would be a wanted Ritz value and the iteration could not converge."""
+    return _lib.GNN_OUT if nev <= 8 else (nev + 15) // 8 * 8
+
+
 def eigen_opts(nev, tol=1e-6, precision="plain", degree=16, max_iters=300):
     o = eigen_options()
     o.init(nev)
-    o.block_size = _lib.GNN_OUT
+    o.block_size = block_size_for(nev)
     o.which = "LA"
     o.tol = tol
     o.precision = precision
@@ -162,7 +179,7 @@ def compare_starts(net, inst, tol=1e-6, precision="plain", seed=0):
     cold = compute_eigen(inst.op, True, opts)
     torch.cuda.synchronize()
     t1 = time.perf_counter()
-    X0 = net.start_block(inst.op, seed)
+    X0 = net.start_block(inst.op, seed, opts.block_size)
     warm = compute_eigen(inst.op, True, opts, X0=X0)
     torch.cuda.synchronize()
     t2 = time.perf_counter()
