@@ -101,6 +101,7 @@ _SIGS = {
     "fmx_eigen_default_options": (None, [_P(eigen_options_t), _int]),
     "fmx_eigen_solve": (_int, [_vp, _vp, _P(eigen_options_t), _vp, _vp, _i64, _vp, _P(eigen_status_t), _vp]),
     "fmx_na_scale": (_int, [_vp, _vp, _vp]),
+    "fmx_pagerank": (_int, [_vp, _u64, C.c_float, _vp, _P(_u64), _vp]),
     "fmx_gnn_create": (_int, [_int, _u64, _P(_vp)]),
     "fmx_gnn_free": (_int, [_vp]),
     "fmx_gnn_set_params": (_int, [_vp, _vp]),

@@ -281,6 +281,18 @@ int fmx_eigen_solve(const fmx_matrix *m, const float *row_scale,
  * of n floats. */
 int fmx_na_scale(const fmx_matrix *m, float *s, void *stream);
 
+/* ---- PageRank ------------------------------------------------------------------
+ * fm::alg::PageRank(mat, max_niters, damping, num_in_mem)
+ * (matrix/libmatrix-algs/PageRank.cpp:63-133) with the reference's float
+ * arithmetic: out-degrees A 1 clamped to >= 1, pr = 1/n, then while fewer than
+ * n vertices changed by less than 0.001/n and fewer than max_iters iterations
+ * ran: in = pr / deg, out = A^T in, pr = out * damping + (1 - damping) / n.
+ * `m` needs its transpose (an asymmetric matrix created with t_img, or a
+ * symmetric one).  pr: n device floats (the result); *iters: iterations run.
+ * Synchronises the stream once per iteration (the convergence test). */
+int fmx_pagerank(const fmx_matrix *m, uint64_t max_iters, float damping, float *pr,
+                 uint64_t *iters, void *stream);
+
 /* ---- learned warm start ---------------------------------------------------------
  * A 2-layer graph network that maps vertex features to a start block for
  * fmx_eigen_solve (no counterpart in the reference):

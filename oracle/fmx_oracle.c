@@ -724,7 +724,9 @@ int orc_pagerank(const char *idx, size_t idx_len, const char *mat, size_t mat_le
 	float *pr = malloc(sizeof(float) * n), *in = malloc(sizeof(float) * n), *out = malloc(sizeof(float) * n);
 	for (uint64_t i = 0; i < n; i++) one[i] = 1.0f;
 	if (orc_spmm(idx, idx_len, mat, mat_len, D_F32, one, deg, 1, nthreads, 0, 0, 0, 0, 0)) return -1;
-	for (uint64_t i = 0; i < n; i++) { if (deg[i] < 1.0f) deg[i] = 1.0f; pr[i] = 1.0f / n; }
+	/* pr = 1.0 / num_vertices in double, stored as float (mat_init_operate, :31-47) */
+	const float p0 = (float)(1.0 / (double)n);
+	for (uint64_t i = 0; i < n; i++) { if (deg[i] < 1.0f) deg[i] = 1.0f; pr[i] = p0; }
 	const float eps = (float)(0.001 / (double)n);          /* :94 */
 	const float teleport = (float)((1.0 - (double)damping) / (double)n); /* :117 */
 	uint64_t converge = 0, it = 0;

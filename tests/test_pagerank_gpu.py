@@ -1,0 +1,67 @@
+"""GPU PageRank (fmx_pagerank) against the oracle's restatement of
+fm::alg::PageRank (matrix/libmatrix-algs/PageRank.cpp:63-133).
+
+Bar: bit-identical ranks and the same iteration count when every vertex's
+in-degree row has at most EXACT_ROW_MAX entries (all sums in the reference's
+order); otherwise rows above that are summed in chunks, so ranks match within
+RTOL = 1e-5 relative and the iteration count may differ by one.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from flashx_b200 import _lib, create_2d_matrix
+from flashx_b200.algs import PageRank
+from flashx_b200.graphs import rmat_edges
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-5
+
+
+def _directed(n, m, seed):
+    rng = np.random.default_rng(seed)
+    return rng.integers(0, n, m).astype(np.uint32), rng.integers(0, n, m).astype(np.uint32)
+
+
+@pytest.mark.parametrize("iters,damping", [(30, 0.85), (5, 0.5), (200, 0.85)])
+def test_pagerank_bit_exact_on_short_rows(torch_cuda, iters, damping):
+    n = 6000
+    src, dst = _directed(n, 50000, 11)
+    m, img, timg = create_2d_matrix(src, dst, None, block_size=(1024, 1024), is_sym=False, nrows=n, ncols=n,
+                                    return_images=True)
+    (idx, mat), (tidx, tmat) = img.bytes(), timg.bytes()
+    assert np.bincount(dst, minlength=n).max() <= _lib.EXACT_ROW_MAX
+    pr, it = PageRank(m, iters, damping)
+    ref, rit = oracle.pagerank(idx, mat, tidx, tmat, iters, damping, nthreads=4)
+    assert it == rit
+    assert np.array_equal(pr.cpu().numpy(), ref)
+
+
+def test_pagerank_rmat_s16_configuration(torch_cuda):
+    """The reference's CPU configuration: R-MAT scale 16, 30 iterations at
+    damping 0.85 (hub rows longer than EXACT_ROW_MAX are summed in chunks)."""
+    from flashx_b200 import set_deduplicate
+    n = 1 << 16
+    src, dst = rmat_edges(16, seed=1)
+    set_deduplicate(True)
+    try:
+        m, img, timg = create_2d_matrix(src, dst, None, block_size=(16384, 16384), is_sym=False, nrows=n, ncols=n,
+                                        return_images=True)
+    finally:
+        set_deduplicate(False)
+    (idx, mat), (tidx, tmat) = img.bytes(), timg.bytes()
+    pr, it = PageRank(m, 30, 0.85)
+    ref, rit = oracle.pagerank(idx, mat, tidx, tmat, 30, 0.85, nthreads=8)
+    assert abs(it - rit) <= 1
+    p = pr.cpu().numpy()
+    np.testing.assert_allclose(p, ref, rtol=RTOL, atol=RTOL * float(ref.max()))
+    assert abs(float(p.astype(np.float64).sum()) - float(ref.astype(np.float64).sum())) < 1e-4
+
+
+def test_pagerank_errors(torch_cuda):
+    from flashx_b200 import FmxError, matrix_image, sparse_matrix
+    rect = sparse_matrix.create(matrix_image.build([0, 1], [1, 0], None, nrows=4, ncols=2, block_size=(2, 2)), None)
+    with pytest.raises(FmxError) as e:
+        PageRank(rect, 10, 0.85)
+    assert e.value.code == _lib.FMX_ERR_DIM
