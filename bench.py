@@ -19,7 +19,9 @@ eigenpairs of D^-1/2 A D^-1/2 of the symmetrised R-MAT scale 22 graph, block
 16, residual 1e-6, plain against mixed precision and against mixed precision
 started from the learned warm start (weights in
 flashx_b200/warmstart_weights.f32), plus that comparison on held-out SBM
-graphs.
+graphs.  The "pagerank" object times fm::alg::PageRank (30 iterations, damping
+0.85) at the reference's CPU configuration (R-MAT scale 16) on the GPU next
+to the oracle's CPU restatement, and at scale 22 on the GPU.
 
 --impl reference times the reference's CPU SpMM algorithm (the oracle's C
 restatement of FlashMatrix's 2D traversal; the reference library itself
@@ -220,11 +222,13 @@ def _timed_solve(torch, dev, fn, reps=3):
         e1.record(stream)
         torch.cuda.synchronize(dev)
         times.append(e0.elapsed_time(e1))
+    _timed_solve.last_times = [round(t, 2) for t in times]
     return float(np.median(times)), res
 
 
 def _solve_summary(ms, r):
-    return {"ms": round(ms, 2), "spmm_calls": int(r.status.spmm_calls), "num_ops": int(r.status.num_ops),
+    return {"ms": round(ms, 2), "ms_each": list(getattr(_timed_solve, "last_times", [])),
+            "spmm_calls": int(r.status.spmm_calls), "num_ops": int(r.status.num_ops),
             "iters": int(r.status.num_iters), "converged": int(r.status.converged),
             "max_residual": float(r.status.max_residual)}
 
@@ -286,6 +290,44 @@ def eigen_measure(a, dev):
         "mixed_learned_ms_median": round(float(np.median(R[:, 2])), 2),
         "plain_random_spmm_sum": int(R[:, 1].sum()), "mixed_learned_spmm_sum": int(R[:, 3].sum()),
         "speedup_total_time": round(float(R[:, 0].sum() / R[:, 2].sum()), 3), "all_converged": int(R[:, 4].sum())}
+    return out
+
+
+def pagerank_measure(a, dev):
+    """PageRank at the reference's CPU configuration (R-MAT scale 16, edge
+    factor 16, seed 1, deduplicated, directed; 30 iterations at damping 0.85)
+    on the GPU against the oracle's restatement of the reference on all host
+    cores, plus the GPU at scale 22; ms per iteration."""
+    import torch
+    from flashx_b200 import create_2d_matrix, set_deduplicate
+    from flashx_b200.algs import PageRank
+    from flashx_b200.graphs import rmat_edges
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    out = {"iterations_max": 30, "damping": 0.85}
+    nthreads, _ = cpu_info()
+    set_deduplicate(True)
+    try:
+        for scale in (16, 22):
+            n = 1 << scale
+            s, d = rmat_edges(scale, seed=1)
+            m, img, timg = create_2d_matrix(s, d, None, block_size=(16384, 16384), is_sym=False, nrows=n, ncols=n,
+                                            return_images=True, device=dev.index)
+            del s, d
+            ms, (pr, it) = _timed_solve(torch, dev, lambda: PageRank(m, 30, 0.85), reps=3)
+            row = {"n": n, "nnz": int(m.get_nnz()), "iters": int(it), "gpu_ms_per_iter": round(ms / max(it, 1), 4)}
+            if scale == 16:
+                (idx, mat), (tidx, tmat) = img.bytes(), timg.bytes()
+                t = time.perf_counter()
+                ref, rit = oracle.pagerank(idx, mat, tidx, tmat, 30, 0.85, nthreads=nthreads)
+                cpu_s = time.perf_counter() - t
+                row.update({"cpu_ms_per_iter": round(cpu_s * 1e3 / max(rit, 1), 3), "cpu_iters": int(rit),
+                            "cpu_cores": nthreads, "cpu_kind": "port",
+                            "max_rel_diff_vs_cpu": float(np.max(np.abs(pr.cpu().numpy() - ref)) / float(ref.max()))})
+            out[f"rmat-s{scale}"] = row
+            del m, img, timg
+    finally:
+        set_deduplicate(False)
     return out
 
 
@@ -425,11 +467,12 @@ def main():
         cpu = {"value": round(gbs[0], 3), "unit": "GB/s", "cores": nthreads, "kind": "port",
                "sample": sample + f"; CPU: {model}"}
 
-    eig = None
+    eig = prk = None
     if rank == 0 and not a.skip_eigen:
         del m, X, Y
         torch.cuda.empty_cache()
         eig = eigen_measure(a, dev)
+        prk = pagerank_measure(a, dev)
 
     if rank == 0:
         line = {
@@ -456,6 +499,7 @@ def main():
             "gpu_launches": a.steps * kernels,
             "clocks": clk,
             "eigen": eig,
+            "pagerank": prk,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

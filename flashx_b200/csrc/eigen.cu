@@ -468,16 +468,17 @@ struct solver {
 		ECUDA_TRY(cudaMemcpyAsync(eye, I.data(), I.size() * sizeof(double), cudaMemcpyHostToDevice, st));
 		ECUDA_TRY(cudaMemsetAsync(tc_err, 0, sizeof(int), st));
 		ECUDA_TRY(cudaMemsetAsync(info, 0, 4 * sizeof(int), st));
-		ECUDA_TRY(cudaMallocHost(&hsmall, sizeof(small_out)));
+		// pinned, once per host thread (a page-locked allocation per solve can
+		// stall for a long time in a process that holds much pinned memory)
+		static thread_local small_out *pinned = nullptr;
+		if (!pinned) ECUDA_TRY(cudaMallocHost(&pinned, sizeof(small_out)));
+		hsmall = pinned;
 		return FMX_OK;
 	}
 
 	~solver()
 	{
-		if (hsmall) {
-			cudaStreamSynchronize(st);
-			cudaFreeHost(hsmall);
-		}
+		cudaStreamSynchronize(st);
 	}
 
 	// tensor-core dense products: mixed precision, low-precision phase only
