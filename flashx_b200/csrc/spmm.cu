@@ -578,21 +578,42 @@ __global__ void pack_hot_kernel(const int32_t *hot_col, uint32_t n_hot, const XT
 	}
 }
 
-// Heavy rows: add the chunk partials in chunk order, scale, convert, store.
+// Heavy rows: add the chunk partials, scale, convert, store.  One warp per
+// row.  Each column j is summed by 32 / kp2 lanes (kp2 = k rounded up to a
+// power of two, at most 32); lane part p takes chunks p, p + parts, ... into
+// two running sums, and the parts are combined by a fixed xor tree: a
+// deterministic order with many loads in flight (the chunk sums of a long
+// row are otherwise one chain of dependent loads).
 template <class YT, class A, bool SCALE_OUT>
 __global__ void spmm_fixup_kernel(const heavy_row *heavy, uint32_t n_heavy, const A *partial,
 		YT *Y, int64_t ldy, int k, const A *s_out)
 {
 	const uint64_t w = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
 	const int lane = threadIdx.x & 31;
-	if (w >= n_heavy) return;
+	if (w >= n_heavy) return;                       // whole warps leave together
 	const heavy_row h = heavy[w];
-	for (int j = lane; j < k; j += 32) {
-		A s = partial[int64_t(h.first) * kPartialStride + j];
-		for (uint32_t c = 1; c < h.count; c++)
-			s = acc_add(s, partial[int64_t(h.first + c) * kPartialStride + j]);
-		if constexpr (SCALE_OUT) s = acc_mul(s, s_out[h.row]);
-		Y[int64_t(h.row) * ldy + j] = from_acc<YT, A>(s);
+	int kp2 = 1;
+	while (kp2 < k && kp2 < 32) kp2 <<= 1;
+	const int parts = 32 / kp2;
+	const int part = lane / kp2, jl = lane % kp2;
+	for (int j0 = 0; j0 < k; j0 += kp2) {
+		const int j = j0 + jl;
+		A s0 = A(0), s1 = A(0);
+		if (j < k) {
+			const A *pc = partial + int64_t(h.first) * kPartialStride + j;
+			uint32_t c = uint32_t(part);
+			for (; c + uint32_t(parts) < h.count; c += 2u * uint32_t(parts)) {
+				s0 = acc_add(s0, pc[int64_t(c) * kPartialStride]);
+				s1 = acc_add(s1, pc[int64_t(c + parts) * kPartialStride]);
+			}
+			if (c < h.count) s0 = acc_add(s0, pc[int64_t(c) * kPartialStride]);
+		}
+		A s = acc_add(s0, s1);
+		for (int o = kp2; o < 32; o <<= 1) s = acc_add(s, __shfl_xor_sync(0xffffffffu, s, o));
+		if (part == 0 && j < k) {
+			if constexpr (SCALE_OUT) s = acc_mul(s, s_out[h.row]);
+			Y[int64_t(h.row) * ldy + j] = from_acc<YT, A>(s);
+		}
 	}
 }
 
