@@ -220,12 +220,46 @@ tc_gemm_kernel(const float *__restrict__ X, int64_t ldx, int K, const float *__r
 	uint32_t phase = 0;
 	bool ok = true;
 	const int64_t ntiles = (n + kTile - 1) / kTile;
+	// fast path: whole 16-byte units of aligned rows, no padding along K
+	const bool vx = Kp == K && (ldx % 4) == 0 && (reinterpret_cast<uintptr_t>(X) & 15) == 0;
+	const bool vy = (N % 4) == 0 && (ldy % 4) == 0 && (reinterpret_cast<uintptr_t>(Y) & 15) == 0;
 	for (int64_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
 		const int64_t row = t * kTile + tid;
-		float v[64];
-		for (int k = 0; k < Kp; k++) v[k] = (row < n && k < K) ? X[row * ldx + k] : 0.f;
-		for (int part = 0; part < C::PARTS; part++)
-			put_units<TF32>(sa + part * a_bytes, kTile * 16, tid, v, Kp, Kp, part);
+		if (vx) {
+			const float4 *xr = reinterpret_cast<const float4 *>(X + row * ldx);
+			for (int u = 0; u < Kp / C::E; u++) {
+				uint32_t w0[4], w1[4];
+				if constexpr (TF32) {
+					const float4 x = row < n ? xr[u] : make_float4(0.f, 0.f, 0.f, 0.f);
+					const float xs[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+					for (int i = 0; i < 4; i++) {
+						const float hi = tf32_round(xs[i]);
+						w0[i] = __float_as_uint(hi);
+						w1[i] = __float_as_uint(tf32_round(xs[i] - hi));
+					}
+				} else {
+					const float4 a = row < n ? xr[2 * u] : make_float4(0.f, 0.f, 0.f, 0.f);
+					const float4 c = row < n ? xr[2 * u + 1] : make_float4(0.f, 0.f, 0.f, 0.f);
+					const float xs[8] = {a.x, a.y, a.z, a.w, c.x, c.y, c.z, c.w};
+#pragma unroll
+					for (int i = 0; i < 4; i++) {
+						__nv_bfloat162 h = __floats2bfloat162_rn(xs[2 * i], xs[2 * i + 1]);
+						memcpy(&w0[i], &h, 4);
+					}
+				}
+				*reinterpret_cast<uint4 *>(sa + size_t(u) * kTile * 16 + size_t(tid) * 16) =
+						make_uint4(w0[0], w0[1], w0[2], w0[3]);
+				if constexpr (TF32)
+					*reinterpret_cast<uint4 *>(sa + a_bytes + size_t(u) * kTile * 16 + size_t(tid) * 16) =
+							make_uint4(w1[0], w1[1], w1[2], w1[3]);
+			}
+		} else {
+			float v[64];
+			for (int k = 0; k < Kp; k++) v[k] = (row < n && k < K) ? X[row * ldx + k] : 0.f;
+			for (int part = 0; part < C::PARTS; part++)
+				put_units<TF32>(sa + part * a_bytes, kTile * 16, tid, v, Kp, Kp, part);
+		}
 		fence_async_smem();
 		__syncthreads();
 		if (tid == 0) {
@@ -254,8 +288,15 @@ tc_gemm_kernel(const float *__restrict__ X, int64_t ldx, int K, const float *__r
 			for (int c0 = 0; c0 < Np; c0 += 16) {
 				float o[16];
 				tmem_ld16(tmem + (uint32_t(warp * 32) << 16) + uint32_t(c0), o);
-				if (r < n)
-					for (int i = 0; i < 16 && c0 + i < N; i++) Y[r * ldy + c0 + i] = o[i];
+				if (r < n) {
+					if (vy && c0 + 16 <= N) {
+						float4 *yr = reinterpret_cast<float4 *>(Y + r * ldy + c0);
+#pragma unroll
+						for (int q = 0; q < 4; q++) yr[q] = make_float4(o[4 * q], o[4 * q + 1], o[4 * q + 2], o[4 * q + 3]);
+					} else {
+						for (int i = 0; i < 16 && c0 + i < N; i++) Y[r * ldy + c0 + i] = o[i];
+					}
+				}
 			}
 		}
 		tc_fence_before();
@@ -417,13 +458,19 @@ tc_gram_kernel(const float *__restrict__ X, int64_t ldx, int M, const float *__r
 	if (warp == 0) tmem_dealloc(tmem, ncols);
 }
 
+// G[i] = sum over the partials of part[p][i]: one warp per element, lane l
+// adding partials l, l + 32, ... and the lanes combined by a fixed xor tree
+// (deterministic for a given number of partials)
 template <class T>
 __global__ void gram_reduce_kernel(const T *part, int nparts, int MN, T *G)
 {
-	for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < MN; i += gridDim.x * blockDim.x) {
+	const int lane = threadIdx.x & 31;
+	const int warps = int((gridDim.x * blockDim.x) >> 5);
+	for (int i = int((blockIdx.x * blockDim.x + threadIdx.x) >> 5); i < MN; i += warps) {
 		T s = 0;
-		for (int p = 0; p < nparts; p++) s += part[size_t(p) * MN + i];
-		G[i] = s;
+		for (int p = lane; p < nparts; p += 32) s += part[size_t(p) * MN + i];
+		for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+		if (lane == 0) G[i] = s;
 	}
 }
 
@@ -671,15 +718,17 @@ int fmx_dense_gemm(int precision, const float *X, int64_t ldx, int64_t n, int K,
 	int dev = 0;
 	cudaGetDevice(&dev);
 	const int64_t tiles = (n + kTile - 1) / kTile;
-	const unsigned grid = unsigned(std::max<int64_t>(1, std::min<int64_t>(tiles, int64_t(sms(dev)) * 4)));
+	// as many CTAs per SM as registers and shared memory allow, but no more
+	// than the SM's 512 TMEM columns hold (each CTA allocates tmem_cols)
+	const int tmem_cols = Np <= 32 ? 32 : (Np <= 64 ? 64 : 128);
+	auto kern = tf32 ? tc_gemm_kernel<true> : tc_gemm_kernel<false>;
+	DCUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+	int per_sm = 0;
+	DCUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, smem));
+	per_sm = std::max(1, std::min(per_sm, 512 / tmem_cols));
+	const unsigned grid = unsigned(std::max<int64_t>(1, std::min<int64_t>(tiles, int64_t(sms(dev)) * per_sm)));
 	cudaStream_t st = static_cast<cudaStream_t>(stream);
-	if (tf32) {
-		DCUDA_TRY(cudaFuncSetAttribute(tc_gemm_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-		tc_gemm_kernel<true><<<grid, 128, smem, st>>>(X, ldx, K, B, ldb, N, Y, ldy, n, err);
-	} else {
-		DCUDA_TRY(cudaFuncSetAttribute(tc_gemm_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-		tc_gemm_kernel<false><<<grid, 128, smem, st>>>(X, ldx, K, B, ldb, N, Y, ldy, n, err);
-	}
+	kern<<<grid, 128, smem, st>>>(X, ldx, K, B, ldb, N, Y, ldy, n, err);
 	DCUDA_TRY(cudaGetLastError());
 	return FMX_OK;
 }
@@ -703,7 +752,7 @@ int fmx_dense_gram(int precision, const float *X, int64_t ldx, int M, const floa
 	if (precision == FMX_DENSE_F64) {
 		gram_f64_kernel<<<parts, 256, 0, st>>>(X, ldx, M, W, ldw, N, n, static_cast<double *>(part));
 		DCUDA_TRY(cudaGetLastError());
-		gram_reduce_kernel<double><<<(M * N + 255) / 256, 256, 0, st>>>(static_cast<const double *>(part), parts, M * N,
+		gram_reduce_kernel<double><<<(M * N + 7) / 8, 256, 0, st>>>(static_cast<const double *>(part), parts, M * N,
 				static_cast<double *>(G));
 		DCUDA_TRY(cudaGetLastError());
 		return FMX_OK;
@@ -722,7 +771,7 @@ int fmx_dense_gram(int precision, const float *X, int64_t ldx, int M, const floa
 		tc_gram_kernel<false><<<parts, 128, smem, st>>>(X, ldx, M, W, ldw, N, n, static_cast<float *>(part), err);
 	}
 	DCUDA_TRY(cudaGetLastError());
-	gram_reduce_kernel<float><<<(M * N + 255) / 256, 256, 0, st>>>(static_cast<const float *>(part), parts, M * N,
+	gram_reduce_kernel<float><<<(M * N + 7) / 8, 256, 0, st>>>(static_cast<const float *>(part), parts, M * N,
 			static_cast<float *>(G));
 	DCUDA_TRY(cudaGetLastError());
 	return FMX_OK;

@@ -70,6 +70,7 @@ namespace fmx {
 constexpr uint32_t kExactMax = FMX_EXACT_ROW_MAX;  // rows summed by one lane group
 constexpr uint32_t kChunk = 256;        // most entries per chunk of a longer row
 constexpr uint32_t kRange = 256;        // target entries per multi-row range
+constexpr uint32_t kLongChunks = 8;     // heavy rows with more chunks get a warp each in the fixup
 #ifndef FMX_HOT_MAX
 #define FMX_HOT_MAX (1u << 20)
 #endif
@@ -121,6 +122,7 @@ struct gpu_part {
 	uint32_t n_ranges = 0;
 	heavy_row *heavy = nullptr;
 	uint32_t n_heavy = 0;
+	uint32_t n_long_heavy = 0;           // the first heavy rows, of more than kLongChunks chunks
 	uint32_t n_partials = 0;
 	void *partial = nullptr;
 	uint64_t hot_entries = 0;            // entries that read the hot pack
@@ -578,43 +580,105 @@ __global__ void pack_hot_kernel(const int32_t *hot_col, uint32_t n_hot, const XT
 	}
 }
 
-// Heavy rows: add the chunk partials, scale, convert, store.  One warp per
-// row.  Each column j is summed by 32 / kp2 lanes (kp2 = k rounded up to a
-// power of two, at most 32); lane part p takes chunks p, p + parts, ... into
-// two running sums, and the parts are combined by a fixed xor tree: a
-// deterministic order with many loads in flight (the chunk sums of a long
-// row are otherwise one chain of dependent loads).
+// Heavy rows: add the chunk partials, scale, convert, store.  A row's
+// columns are covered by L lanes (L = k / 4 float4 lanes for FP32 panels of
+// k % 4 == 0, else one lane per column, rounded up to a power of two, at most
+// 32) and its chunks by P parts: part q adds chunks q, q + P, ... into two
+// running sums, and the parts are combined by a fixed xor tree.  The heavy
+// rows come longest first: each of the first n_long rows (more than
+// kLongChunks chunks) gets a warp with P = 32 / L; the rest go 32 / (2 L)
+// rows to a warp with P = 2 (one row and P = 1 when L = 32).  Deterministic,
+// with many loads in flight.
 template <class YT, class A, bool SCALE_OUT>
-__global__ void spmm_fixup_kernel(const heavy_row *heavy, uint32_t n_heavy, const A *partial,
-		YT *Y, int64_t ldy, int k, const A *s_out)
+__global__ void spmm_fixup_kernel(const heavy_row *heavy, uint32_t n_heavy, uint32_t n_long, const A *partial,
+		YT *Y, int64_t ldy, int k, const A *s_out, int L)
 {
+	constexpr bool kVec4 = std::is_same<A, float>::value;
+	const bool vec = kVec4 && (k % 4) == 0;
+	const int units = vec ? k / 4 : k;
 	const uint64_t w = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
 	const int lane = threadIdx.x & 31;
-	if (w >= n_heavy) return;                       // whole warps leave together
-	const heavy_row h = heavy[w];
-	int kp2 = 1;
-	while (kp2 < k && kp2 < 32) kp2 <<= 1;
-	const int parts = 32 / kp2;
-	const int part = lane / kp2, jl = lane % kp2;
-	for (int j0 = 0; j0 < k; j0 += kp2) {
-		const int j = j0 + jl;
-		A s0 = A(0), s1 = A(0);
-		if (j < k) {
-			const A *pc = partial + int64_t(h.first) * kPartialStride + j;
+	const bool long_rows = w < n_long;
+	const int P = long_rows ? 32 / L : (L < 32 ? 2 : 1);
+	const int lanes = L * P;                          // per row
+	const uint64_t r = long_rows ? w : uint64_t(n_long) + (w - n_long) * uint64_t(32 / lanes) + uint64_t(lane / lanes);
+	const int sub = lane % lanes, part = sub / L, cl = sub % L;
+	const bool live = r < n_heavy;
+	heavy_row h{0, 0, 0};
+	if (live) h = heavy[r];
+	for (int u0 = 0; u0 < units; u0 += L) {           // the same trip count on every lane
+		const int u = u0 + cl;
+		const bool mine = live && u < units;
+		A s0[4] = {A(0), A(0), A(0), A(0)}, s1[4] = {A(0), A(0), A(0), A(0)};
+		if (mine) {
+			const A *pc = partial + int64_t(h.first) * kPartialStride + (vec ? 4 * u : u);
 			uint32_t c = uint32_t(part);
-			for (; c + uint32_t(parts) < h.count; c += 2u * uint32_t(parts)) {
-				s0 = acc_add(s0, pc[int64_t(c) * kPartialStride]);
-				s1 = acc_add(s1, pc[int64_t(c + parts) * kPartialStride]);
+			for (; c + uint32_t(P) < h.count; c += 2u * uint32_t(P)) {
+				if constexpr (kVec4) {
+					if (vec) {
+						const float4 a = *reinterpret_cast<const float4 *>(pc + int64_t(c) * kPartialStride);
+						const float4 b = *reinterpret_cast<const float4 *>(pc + int64_t(c + P) * kPartialStride);
+						s0[0] = acc_add(s0[0], a.x); s0[1] = acc_add(s0[1], a.y);
+						s0[2] = acc_add(s0[2], a.z); s0[3] = acc_add(s0[3], a.w);
+						s1[0] = acc_add(s1[0], b.x); s1[1] = acc_add(s1[1], b.y);
+						s1[2] = acc_add(s1[2], b.z); s1[3] = acc_add(s1[3], b.w);
+						continue;
+					}
+				}
+				s0[0] = acc_add(s0[0], pc[int64_t(c) * kPartialStride]);
+				s1[0] = acc_add(s1[0], pc[int64_t(c + P) * kPartialStride]);
 			}
-			if (c < h.count) s0 = acc_add(s0, pc[int64_t(c) * kPartialStride]);
+			if (c < h.count) {
+				if constexpr (kVec4) {
+					if (vec) {
+						const float4 a = *reinterpret_cast<const float4 *>(pc + int64_t(c) * kPartialStride);
+						s0[0] = acc_add(s0[0], a.x); s0[1] = acc_add(s0[1], a.y);
+						s0[2] = acc_add(s0[2], a.z); s0[3] = acc_add(s0[3], a.w);
+					} else {
+						s0[0] = acc_add(s0[0], pc[int64_t(c) * kPartialStride]);
+					}
+				} else {
+					s0[0] = acc_add(s0[0], pc[int64_t(c) * kPartialStride]);
+				}
+			}
 		}
-		A s = acc_add(s0, s1);
-		for (int o = kp2; o < 32; o <<= 1) s = acc_add(s, __shfl_xor_sync(0xffffffffu, s, o));
-		if (part == 0 && j < k) {
-			if constexpr (SCALE_OUT) s = acc_mul(s, s_out[h.row]);
-			Y[int64_t(h.row) * ldy + j] = from_acc<YT, A>(s);
+		const int nv = vec ? 4 : 1;
+		A t[4];
+#pragma unroll
+		for (int i = 0; i < 4; i++) t[i] = acc_add(s0[i], s1[i]);
+		for (int o = L; o < lanes; o <<= 1)
+#pragma unroll
+			for (int i = 0; i < 4; i++) t[i] = acc_add(t[i], __shfl_xor_sync(0xffffffffu, t[i], o));
+		if (mine && part == 0) {
+			A so = A(1);
+			if constexpr (SCALE_OUT) so = s_out[h.row];
+			YT *y = Y + int64_t(h.row) * ldy + (vec ? 4 * u : u);
+			for (int i = 0; i < nv; i++) {
+				A v = t[i];
+				if constexpr (SCALE_OUT) v = acc_mul(v, so);
+				y[i] = from_acc<YT, A>(v);
+			}
 		}
 	}
+}
+
+template <class YT, class A, bool SCALE_OUT>
+static int launch_fixup(const gpu_part &p, const A *partial, YT *Y, int64_t ldy, int k, const A *s_out,
+		cudaStream_t st)
+{
+	if (!p.n_heavy) return FMX_OK;
+	const bool vec = std::is_same<A, float>::value && (k % 4) == 0;
+	const int units = vec ? k / 4 : k;
+	int L = 1;
+	while (L < units && L < 32) L <<= 1;
+	const uint64_t n_short = p.n_heavy - p.n_long_heavy;
+	const uint64_t per_warp = uint64_t(32 / (L * (L < 32 ? 2 : 1)));    // short rows per warp
+	const uint64_t warps = p.n_long_heavy + (n_short + per_warp - 1) / per_warp;
+	const unsigned fb = unsigned((warps * 32 + 255) / 256);
+	spmm_fixup_kernel<YT, A, SCALE_OUT><<<fb, 256, 0, st>>>(p.heavy, p.n_heavy, p.n_long_heavy, partial, Y, ldy,
+			k, s_out, L);
+	CUDA_TRY(cudaGetLastError());
+	return FMX_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -795,6 +859,11 @@ static int make_part(const host_csr &csr, int device, std::shared_ptr<gpu_part> 
 	}
 	if (!rc) rc = upload(&p->hot_col, hot_col.data(), hot_col.size(), bytes);
 	if (!rc) rc = upload(&p->ranges, ranges.data(), ranges.size(), bytes);
+	// longest first (the fixup gives each long row a warp and packs the short
+	// ones several to a warp); ties keep row order
+	std::stable_sort(heavy.begin(), heavy.end(), [](const heavy_row &x, const heavy_row &y) { return x.count > y.count; });
+	p->n_long_heavy = uint32_t(std::count_if(heavy.begin(), heavy.end(),
+			[](const heavy_row &h) { return h.count > kLongChunks; }));
 	if (!rc) rc = upload(&p->heavy, heavy.data(), heavy.size(), bytes);
 	p->n_hot = uint32_t(hot_col.size());
 	p->n_exact = n_exact;
@@ -865,14 +934,11 @@ static int launch_t(const gpu_part &p, spmm_args a, bool sin, bool sout, cudaStr
 	else if (sout) rc = launch_one<XT, YT, A, WT, VEC, NV, false, true>(p, a, st);
 	else rc = launch_one<XT, YT, A, WT, VEC, NV, false, false>(p, a, st);
 	if (rc) return rc;
-	if (p.n_heavy) {
-		unsigned fb = unsigned((uint64_t(p.n_heavy) * 32 + 255) / 256);
-		if (sout) spmm_fixup_kernel<YT, A, true><<<fb, 256, 0, st>>>(p.heavy, p.n_heavy, static_cast<const A *>(a.partial),
-				static_cast<YT *>(a.Y), a.ldy, a.k, static_cast<const A *>(a.s_out));
-		else spmm_fixup_kernel<YT, A, false><<<fb, 256, 0, st>>>(p.heavy, p.n_heavy, static_cast<const A *>(a.partial),
-				static_cast<YT *>(a.Y), a.ldy, a.k, static_cast<const A *>(a.s_out));
-		CUDA_TRY(cudaGetLastError());
-	}
+	if (sout) rc = launch_fixup<YT, A, true>(p, static_cast<const A *>(a.partial), static_cast<YT *>(a.Y), a.ldy, a.k,
+			static_cast<const A *>(a.s_out), st);
+	else rc = launch_fixup<YT, A, false>(p, static_cast<const A *>(a.partial), static_cast<YT *>(a.Y), a.ldy, a.k,
+			nullptr, st);
+	if (rc) return rc;
 	return FMX_OK;
 }
 
@@ -1334,12 +1400,9 @@ static int run_noalloc(const gpu_part &p, const float *X, int64_t ldx, float *Y,
 			rc = launch_one<float, float, float, WT, 1, 4, false, false>(p, a, st);
 		}
 		if (rc) return rc;
-		if (p.n_heavy) {
-			unsigned fb = unsigned((uint64_t(p.n_heavy) * 32 + 255) / 256);
-			spmm_fixup_kernel<float, float, false><<<fb, 256, 0, st>>>(p.heavy, p.n_heavy,
-					static_cast<const float *>(partial), Y + c0, ldy, kp, nullptr);
-			CUDA_TRY(cudaGetLastError());
-		}
+		const int frc = launch_fixup<float, float, false>(p, static_cast<const float *>(partial), Y + c0, ldy, kp,
+				nullptr, st);
+		if (frc) return frc;
 	}
 	return FMX_OK;
 }

@@ -230,9 +230,9 @@ int fmx_dense_sym_eig(const double *H, int b, double *w, double *V, void *stream
 #define FMX_EIGEN_PLAIN 0   /* FP32 SpMM operands; dense products in FP64 on CUDA cores */
 #define FMX_EIGEN_MIXED 1   /* filter in correction form with BF16 SpMM operands (FP32
                                accumulation), Rayleigh-Ritz SpMM in FP32; CholQR basis
-                               update and Rayleigh quotient on tensor cores (3xTF32)
-                               until tensor_until, FP64 after; CholQR Gram, Cholesky,
-                               projected problem and residual norms in FP64 */
+                               update on tensor cores (3xTF32) until tensor_until, FP64
+                               after; Gram products, Cholesky, projected problem and
+                               residual norms in FP64 */
 
 typedef struct fmx_eigen_options {
 	int nev;            /* wanted eigenpairs (eigen_options::nev) */
