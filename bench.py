@@ -208,7 +208,7 @@ def read_traffic(name):
         return None
 
 
-def _timed_solve(torch, dev, fn, reps=3):
+def _timed_solve(torch, dev, fn, reps=5):
     """Median wall time (ms, CUDA events on the current stream) of `fn`,
     after one untimed call; returns (ms, last result)."""
     fn()
@@ -255,7 +255,7 @@ def eigen_measure(a, dev):
     op = NA_operator(m, device=dev.index)
     out = {"workload": f"rmat-s{a.eig_scale}-ef16-symmetrised-na-top8-block16-tol1e-6", "n": n,
            "nnz": int(m.get_nnz()), "build_s": round(time.time() - t0, 2),
-           "timing": "median of 3 after 1 warm-up, CUDA events around the whole solve (host loop included)"}
+           "timing": "median of 5 after 1 warm-up, CUDA events around the whole solve (host loop included)"}
     for prec in ("plain", "mixed"):
         o = ws.eigen_opts(8, 1e-6, prec)
         ms, r = _timed_solve(torch, dev, lambda: compute_eigen(op, True, o))

@@ -127,8 +127,8 @@ __device__ __forceinline__ void st4(__nv_bfloat16 *p, float4 v)
 	*reinterpret_cast<uint2 *>(p) = u;
 }
 
-template <class ET, class PT, class OT>
-__global__ void corr_kernel(const float *__restrict__ W, const ET *__restrict__ E, const PT *__restrict__ P,
+template <class WT, class ET, class PT, class OT>
+__global__ void corr_kernel(const WT *__restrict__ W, const ET *__restrict__ E, const PT *__restrict__ P,
 		const float *__restrict__ R, const float *__restrict__ X, OT *__restrict__ O, int64_t count, int b,
 		float alpha, float ac0, float beta, col_coefs cf)
 {
@@ -167,7 +167,7 @@ __global__ void corr_kernel(const float *__restrict__ W, const ET *__restrict__ 
 	for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < count; i += tstride) {
 		const int col = pow2 ? int(i & (b - 1)) : int(i % b);
 		float v = 0.f;
-		if (W) v = alpha * W[i];
+		if (W) v = alpha * ldf(W + i);
 		if (E) v -= ac0 * ldf(E + i);
 		if (P) v -= beta * ldf(P + i);
 		if (R) v += cf.r[col] * R[i];
@@ -429,9 +429,9 @@ struct solver {
 	int ritz_grid = 1;
 	int64_t spmm_calls = 0, num_ops = 0;
 
-	int spmm(int xt, const void *Xin, int k, float *Out)
+	int spmm(int xt, const void *Xin, int k, void *Out, int yt = FMX_F32)
 	{
-		E_TRY(fmx_spmm(m, xt, Xin, b, FMX_F32, Out, b, k, s, s, st));
+		E_TRY(fmx_spmm(m, xt, Xin, b, yt, Out, b, k, s, s, st));
 		spmm_calls++;
 		num_ops += k;
 		return FMX_OK;
@@ -606,12 +606,13 @@ struct solver {
 		return FMX_OK;
 	}
 
-	template <class ET, class PT, class OT>
-	int corr_step(const float *Wm, const ET *E, const PT *P, const float *R, const float *Xs, OT *Out, float alpha,
+	template <class WT, class ET, class PT, class OT>
+	int corr_step(const WT *Wm, const ET *E, const PT *P, const float *R, const float *Xs, OT *Out, float alpha,
 			float ac0, float beta, const col_coefs &cf)
 	{
 		const int64_t cnt = n * b;
-		corr_kernel<ET, PT, OT><<<flat_grid(cnt), kThreads, 0, st>>>(Wm, E, P, R, Xs, Out, cnt, b, alpha, ac0, beta, cf);
+		corr_kernel<WT, ET, PT, OT><<<flat_grid(cnt), kThreads, 0, st>>>(Wm, E, P, R, Xs, Out, cnt, b, alpha, ac0, beta,
+				cf);
 		ECUDA_TRY(cudaGetLastError());
 		return FMX_OK;
 	}
@@ -654,7 +655,8 @@ struct solver {
 			const double sn = 1.0 / (2.0 / s1 - sj);
 			const double alpha = 2 * sn / e, beta = sj * sn;
 			const bool last = jdeg == mdeg;
-			E_TRY(spmm(FMX_BF16, B[cur], b, W));
+			// W = A_s E in BF16 too: its rounding is relative to the correction
+			E_TRY(spmm(FMX_BF16, B[cur], b, W, FMX_BF16));
 			for (int j = 0; j < b; j++) {
 				Dn[j] = alpha * (hsmall->theta[j] - c0) * Dc[j] - beta * Dp[j];
 				cf.r[j] = float(alpha * Dc[j]);
@@ -664,8 +666,9 @@ struct solver {
 			const bf *E = (const bf *)B[cur];
 			const bf *P = prev < 0 ? nullptr : (const bf *)B[prev];
 			const float a = float(alpha), ac = float(alpha * c0), bt = float(beta);
-			if (last) E_TRY(corr_step(W, E, P, R, X, B[nxt], a, ac, bt, cf));
-			else E_TRY(corr_step(W, E, P, R, (const float *)nullptr, (bf *)B[nxt], a, ac, bt, cf));
+			const bf *Wb = (const bf *)W;
+			if (last) E_TRY(corr_step(Wb, E, P, R, X, B[nxt], a, ac, bt, cf));
+			else E_TRY(corr_step(Wb, E, P, R, (const float *)nullptr, (bf *)B[nxt], a, ac, bt, cf));
 			prev = cur;
 			cur = nxt;
 			sj = sn;

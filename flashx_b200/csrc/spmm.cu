@@ -81,6 +81,12 @@ constexpr int kThreads = 256;           // threads per SpMM block
 #ifndef FMX_SPMM_MIN_BLOCKS
 #define FMX_SPMM_MIN_BLOCKS 5           // resident blocks per SM the register budget targets
 #endif
+#ifndef FMX_SPMM_MIN_BLOCKS_2B
+#define FMX_SPMM_MIN_BLOCKS_2B 4        // the same for 2-byte (BF16) operands: measured at R-MAT
+                                        // scale 22, k = 16, 4 blocks of more registers beat 5
+                                        // (0.837 against 0.894 ms), while FP32 at scale 24
+                                        // prefers 5 (2.56 against 2.73 ms)
+#endif
 constexpr int kStep = 8;                // entries per index load group (alignment unit)
 constexpr uint32_t kEnd = 0x80000000u;  // last entry of a row
 constexpr uint32_t kHot = 0x40000000u;  // entry refers to a hot slot
@@ -541,7 +547,7 @@ __device__ __forceinline__ void run_range(const spmm_args &a, const range_t rg, 
 }
 
 template <class XT, class YT, class A, class WT, int VEC, int NV, int U, bool SCALE_IN, bool SCALE_OUT>
-__global__ void __launch_bounds__(kThreads, FMX_SPMM_MIN_BLOCKS)
+__global__ void __launch_bounds__(kThreads, sizeof(XT) == 2 ? FMX_SPMM_MIN_BLOCKS_2B : FMX_SPMM_MIN_BLOCKS)
 spmm_kernel(const spmm_args a)
 {
 	const int lane = threadIdx.x & 31;
