@@ -84,6 +84,24 @@ def build_graph(a):
     return img, time.time() - t0
 
 
+def max_over_ranks(x, world, device):
+    """The largest value of x over the ranks (the slowest replica's time);
+    x itself when the job has one rank.  `device` holds the reduction tensor:
+    the rank's GPU under NCCL, the CPU under gloo."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_gbs(bytes_per_step, steps, world, seconds):
+    """Whole-job GB/s: every replica's bytes over the slowest replica's time."""
+    return bytes_per_step * steps * world / seconds / 1e9
+
+
 def b_alg(n_rows, n_cols, nnz, k, weighted, s=4):
     return 4 * (n_rows + 1) + 4 * nnz * (1 + int(weighted)) + n_cols * k * s + n_rows * k * s
 
@@ -424,13 +442,10 @@ def main():
     clk = clocks.stop()
     total_ms = t_begin.elapsed_time(t_end)
     launch_ms = float(np.mean([s.elapsed_time(e) for s, e in zip(starts, ends)]))
-    if world > 1:
-        tt = torch.tensor([total_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total_ms = float(tt.item())
+    total_ms = max_over_ranks(total_ms, world, dev)
 
     per_spmm = b_alg(n_rows, n_cols, nnz, k, a.weighted)
-    value = per_spmm * a.steps * world / (total_ms / 1e3) / 1e9
+    value = job_gbs(per_spmm, a.steps, world, total_ms / 1e3)
     peak, peak_kind = read_peaks()
     achieved = per_spmm / (launch_ms / 1e3) / 1e9
     tr = read_traffic(workload_name(a))
@@ -451,12 +466,8 @@ def main():
         t = time.perf_counter()
         for _ in range(a.e2e_steps):
             m.multiply_host(Xn, Yn)
-        e2e_s = time.perf_counter() - t
-        if world > 1:
-            tt = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            e2e_s = float(tt.item())
-        e2e = {"value": round(per_spmm * a.e2e_steps * world / e2e_s / 1e9, 3), "unit": "GB/s",
+        e2e_s = max_over_ranks(time.perf_counter() - t, world, dev)
+        e2e = {"value": round(job_gbs(per_spmm, a.e2e_steps, world, e2e_s), 3), "unit": "GB/s",
                "h2d_bytes_per_step": n_cols * k * 4, "d2h_bytes_per_step": n_rows * k * 4,
                "ms_per_step": round(e2e_s / a.e2e_steps * 1e3, 3)}
 
