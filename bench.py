@@ -61,6 +61,9 @@ def parse():
     p.add_argument("--skip-eigen", action="store_true")
     p.add_argument("--eig-scale", type=int, default=22, help="R-MAT scale of the eigensolver workload")
     p.add_argument("--eig-sbm", type=int, default=20, help="held-out SBM graphs for the learned warm start")
+    p.add_argument("--large", action="store_true",
+                   help="run only the large single-GPU configuration (R-MAT scale 26: SpMM k=16 and 32, top-16 "
+                        "eigensolve plain / mixed / learned start) and print its JSON line")
     return p.parse_args()
 
 
@@ -349,6 +352,72 @@ def pagerank_measure(a, dev):
     return out
 
 
+def large_run(a):
+    """The large single-GPU configuration: R-MAT scale 26 (edge factor 16,
+    seed 1, deduplicated; int32 column ids), FP32 SpMM at k = 16 and 32 on
+    the directed graph, then the top 16 eigenpairs of D^-1/2 A D^-1/2 of the
+    symmetrised graph (block 24, residual 1e-6): plain, mixed, and mixed from
+    the learned start."""
+    import torch
+    from flashx_b200 import matrix_image, sparse_matrix
+    from flashx_b200.eigen import NA_operator, compute_eigen
+    from flashx_b200.graphs import rmat_edges, symmetrize
+    from flashx_b200 import warmstart as ws
+    dev = torch.device("cuda", 0)
+    scale = 26
+    n = 1 << scale
+    out = {"workload": f"rmat-s{scale}-ef16", "n": n}
+    t = time.time()
+    s, d = rmat_edges(scale, seed=1)
+    img = matrix_image.build(s, d, None, nrows=n, ncols=n, block_size=(16384, 16384), dedup=True)
+    out["directed_build_s"] = round(time.time() - t, 1)
+    t = time.time()
+    m = sparse_matrix.create(img, None)
+    torch.cuda.synchronize()
+    out["create_s"] = round(time.time() - t, 1)
+    nnz = m.get_nnz()
+    out["directed_nnz"] = int(nnz)
+    del img
+    for k in (16, 32):
+        X = torch.randn((n, k), device=dev)
+        Y = torch.empty((n, k), device=dev)
+        for _ in range(5):
+            m.multiply(X, Y)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(50):
+            m.multiply(X, Y)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 50
+        out[f"spmm_k{k}"] = {"ms": round(ms, 3), "gbs": round(b_alg(n, n, nnz, k, False) / ms / 1e6, 1)}
+        del X, Y
+    del m
+    torch.cuda.empty_cache()
+    t = time.time()
+    s, d = symmetrize(s, d)
+    img = matrix_image.build(s, d, None, nrows=n, ncols=n, block_size=(16384, 16384), dedup=True)
+    del s, d
+    m = sparse_matrix.create(img, None)
+    del img
+    op = NA_operator(m)
+    torch.cuda.synchronize()
+    out["symmetrised_build_s"] = round(time.time() - t, 1)
+    out["symmetrised_nnz"] = int(m.get_nnz())
+    net = ws.warm_start_net.load(os.path.join(ROOT, "flashx_b200", "warmstart_weights.f32"))
+    for name, prec, learned in (("plain", "plain", False), ("mixed", "mixed", False),
+                                ("mixed_learned", "mixed", True)):
+        o = ws.eigen_opts(16, 1e-6, prec)
+        ms, r = _timed_solve(torch, dev, lambda: compute_eigen(
+            op, True, o, X0=net.start_block(op, 0, o.block_size) if learned else None), reps=2)
+        out[name] = _solve_summary(ms, r)
+        out[name]["block"] = o.block_size
+        if learned:
+            out[name]["spmm_calls"] += ws.SPMM_PER_START
+    return out
+
+
 def run_reference(a, rank, world):
     if rank != 0:
         return
@@ -383,6 +452,10 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if a.impl == "reference":
         return run_reference(a, rank, world)
+    if a.large:
+        if rank == 0:
+            print(json.dumps(large_run(a)), flush=True)
+        return
 
     import torch
     import torch.distributed as dist

@@ -29,6 +29,7 @@ DENSE_BF16, DENSE_TF32X3, DENSE_F64 = 0, 1, 2
 EIGEN_LA, EIGEN_LM = 0, 1
 GNN_FEATURES, GNN_OUT, GNN_PARAMS = 64, 16, 5184
 EIGEN_PLAIN, EIGEN_MIXED = 0, 1
+EIGEN_OP_SCALED, EIGEN_OP_GRAM = 0, 1
 
 BUILD_DEDUP = 0x1
 BUILD_KEEP_SELF_LOOPS = 0x2
@@ -61,7 +62,7 @@ class eigen_options_t(C.Structure):
     _fields_ = [("nev", C.c_int), ("block_size", C.c_int), ("degree", C.c_int), ("max_iters", C.c_int),
                 ("which", C.c_int), ("precision", C.c_int), ("tol", C.c_double), ("lower", C.c_double),
                 ("upper", C.c_double), ("tensor_until", C.c_double), ("seed", C.c_uint64), ("X0", C.c_void_p),
-                ("ldx0", C.c_int64)]
+                ("ldx0", C.c_int64), ("op", C.c_int)]
 
 
 class eigen_status_t(C.Structure):

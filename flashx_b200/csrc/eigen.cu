@@ -414,6 +414,9 @@ struct small_out {
 
 struct solver {
 	const fmx_matrix *m;
+	fmx_matrix *mt = nullptr;        // the transpose (FMX_EIGEN_OP_GRAM)
+	int64_t nrows = 0;               // rows of A (the Gram operator's intermediate)
+	void *tmp = nullptr;             // A x for the Gram operator: nrows x b
 	const float *s;                  // row scale or null
 	fmx_eigen_options o;
 	int64_t n;
@@ -429,8 +432,19 @@ struct solver {
 	int ritz_grid = 1;
 	int64_t spmm_calls = 0, num_ops = 0;
 
+	// One application of the operator to k columns: diag(s) A diag(s) X, or
+	// A^T (A X) for the Gram operator (the intermediate in the output's type
+	// when the input is BF16, as the SpMM's type pairs require).
 	int spmm(int xt, const void *Xin, int k, void *Out, int yt = FMX_F32)
 	{
+		if (o.op == FMX_EIGEN_OP_GRAM) {
+			const int tt = xt == FMX_BF16 ? yt : FMX_F32;
+			E_TRY(fmx_spmm(m, xt, Xin, b, tt, tmp, b, k, nullptr, nullptr, st));
+			E_TRY(fmx_spmm(mt, tt, tmp, b, yt, Out, b, k, nullptr, nullptr, st));
+			spmm_calls += 2;
+			num_ops += 2 * k;
+			return FMX_OK;
+		}
 		E_TRY(fmx_spmm(m, xt, Xin, b, yt, Out, b, k, s, s, st));
 		spmm_calls++;
 		num_ops += k;
@@ -441,6 +455,11 @@ struct solver {
 	{
 		ws.st = st;
 		const size_t nb = size_t(n) * b;
+		if (o.op == FMX_EIGEN_OP_GRAM) {
+			float *t = nullptr;
+			E_TRY(ws.get(&t, size_t(nrows) * b));
+			tmp = t;
+		}
 		E_TRY(ws.get(&X, nb));
 		E_TRY(ws.get(&NX, nb));
 		E_TRY(ws.get(&W, nb));
@@ -477,6 +496,7 @@ struct solver {
 	~solver()
 	{
 		cudaStreamSynchronize(st);
+		if (mt) fmx_matrix_free(mt);
 	}
 
 	// tensor-core dense products: mixed precision, low-precision phase only
@@ -810,6 +830,7 @@ void fmx_eigen_default_options(fmx_eigen_options *o, int nev)
 	o->seed = 1;
 	o->X0 = nullptr;
 	o->ldx0 = 0;
+	o->op = FMX_EIGEN_OP_SCALED;
 }
 
 int fmx_eigen_solve(const fmx_matrix *m, const float *row_scale, const fmx_eigen_options *opt, double *evals,
@@ -819,13 +840,18 @@ int fmx_eigen_solve(const fmx_matrix *m, const float *row_scale, const fmx_eigen
 	uint64_t nrows = 0, ncols = 0, nnz = 0;
 	int prim = 0;
 	E_TRY(fmx_matrix_info(m, &nrows, &ncols, &nnz, &prim, nullptr));
-	if (nrows != ncols) return set_error(FMX_ERR_DIM, "the eigensolver needs a square matrix (%llu x %llu)",
-			(unsigned long long)nrows, (unsigned long long)ncols);
 	const fmx_eigen_options &o = *opt;
+	if (o.op != FMX_EIGEN_OP_SCALED && o.op != FMX_EIGEN_OP_GRAM)
+		return set_error(FMX_ERR_INVAL, "op: FMX_EIGEN_OP_SCALED or FMX_EIGEN_OP_GRAM");
+	if (o.op == FMX_EIGEN_OP_SCALED && nrows != ncols)
+		return set_error(FMX_ERR_DIM, "the eigensolver needs a square matrix (%llu x %llu)",
+				(unsigned long long)nrows, (unsigned long long)ncols);
+	if (o.op == FMX_EIGEN_OP_GRAM && row_scale)
+		return set_error(FMX_ERR_INVAL, "the Gram operator A^T A takes no row scale");
 	if (o.block_size < 1 || o.block_size > kMaxB) return set_error(FMX_ERR_UNSUPPORTED, "block_size in 1..%d", kMaxB);
 	if (o.nev < 1 || o.nev > o.block_size) return set_error(FMX_ERR_INVAL, "nev in 1..block_size (got %d, %d)", o.nev,
 			o.block_size);
-	if (uint64_t(o.block_size) > nrows) return set_error(FMX_ERR_DIM, "block_size exceeds the matrix size");
+	if (uint64_t(o.block_size) > ncols) return set_error(FMX_ERR_DIM, "block_size exceeds the matrix size");
 	if (o.degree < 1 || o.degree > 100) return set_error(FMX_ERR_INVAL, "degree in 1..100");
 	if (o.which != FMX_EIGEN_LA && o.which != FMX_EIGEN_LM) return set_error(FMX_ERR_INVAL, "which: LA or LM");
 	if (o.precision != FMX_EIGEN_PLAIN && o.precision != FMX_EIGEN_MIXED)
@@ -837,9 +863,11 @@ int fmx_eigen_solve(const fmx_matrix *m, const float *row_scale, const fmx_eigen
 		return set_error(FMX_ERR_TYPE, "the eigensolver takes binary or float-weighted matrices");
 	solver sv;
 	sv.m = m;
-	sv.s = row_scale;
+	if (o.op == FMX_EIGEN_OP_GRAM) E_TRY(fmx_matrix_transpose(m, &sv.mt));
+	sv.nrows = int64_t(nrows);
+	sv.s = o.op == FMX_EIGEN_OP_GRAM ? nullptr : row_scale;
 	sv.o = o;
-	sv.n = int64_t(nrows);
+	sv.n = int64_t(ncols);
 	sv.b = o.block_size;
 	sv.st = static_cast<cudaStream_t>(stream);
 	return sv.run(evals, evecs, ldv, residuals, status);

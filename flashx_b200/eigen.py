@@ -119,18 +119,45 @@ class NA_operator:
         return self.mat.multiply(x, None, self.scale, self.scale)
 
 
+class SVD_operator:
+    """A^T A through the transpose (SVD_Operator, test-eigen.cpp:138-177):
+    its top eigenpairs are the squared singular values and the right
+    singular vectors of A.  The spectrum bound the Chebyshev filter needs is
+    ||A^T A|| <= ||A||_1 ||A||_inf = (max column sum) (max row sum), from two
+    SpMMs with a ones vector (exact as a bound for nonnegative entries)."""
+
+    def __init__(self, mat):
+        import torch
+        self.mat = mat
+        dev = f"cuda:{mat.device}"
+        r = mat.multiply(torch.ones((mat.get_num_cols(), 1), device=dev))
+        c = mat.transpose().multiply(torch.ones((mat.get_num_rows(), 1), device=dev))
+        self.upper = float(r.abs().max()) * float(c.abs().max())
+
+    def get_num_rows(self):
+        return self.mat.get_num_cols()
+
+    def get_num_cols(self):
+        return self.mat.get_num_cols()
+
+
 def compute_eigen(op, sym, opts, X0=None, stream=None):
     """compute_eigen(func, sym, opts) (eigensolver.h:74-75).  `op` is an
-    NA_operator or a symmetric sparse_matrix; X0 an optional start block
-    (n x block_size CUDA FP32 tensor, e.g. a learned warm start)."""
+    NA_operator, an SVD_operator or a symmetric sparse_matrix; X0 an optional
+    start block (n x block_size CUDA FP32 tensor, e.g. a learned warm
+    start)."""
     import torch
     if not sym:
         raise ValueError("the block eigensolver handles symmetric operators")
-    mat = op.mat if isinstance(op, NA_operator) else op
+    gram = isinstance(op, SVD_operator)
+    mat = op.mat if isinstance(op, (NA_operator, SVD_operator)) else op
     scale = op.scale if isinstance(op, NA_operator) else None
-    n = mat.get_num_rows()
+    n = mat.get_num_cols() if gram else mat.get_num_rows()
     o = opts._struct()
-    dev = scale.device if scale is not None else torch.device("cuda", 0)
+    if gram:
+        o.op = _lib.EIGEN_OP_GRAM
+        o.lower, o.upper = 0.0, max(op.upper, 1e-30)
+    dev = scale.device if scale is not None else torch.device("cuda", mat.device)
     if X0 is not None:
         if X0.dtype != torch.float32 or not X0.is_cuda or X0.shape != (n, o.block_size) or X0.stride(1) != 1:
             raise ValueError(f"X0 must be a row-major CUDA float32 tensor of shape ({n}, {o.block_size})")

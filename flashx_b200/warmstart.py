@@ -38,7 +38,7 @@ class warm_start_net:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
+        if h is not None and h.value and lib is not None:     # the module may be torn down at exit
             lib.fmx_gnn_free(h)
             self._h = C.c_void_p(None)
 

@@ -227,6 +227,8 @@ int fmx_dense_sym_eig(const double *H, int b, double *w, double *V, void *stream
  * eigen_res::eigen_status (:51-54). */
 #define FMX_EIGEN_LA 0      /* largest algebraic ("LA") */
 #define FMX_EIGEN_LM 1      /* largest magnitude ("LM", the reference's default) */
+#define FMX_EIGEN_OP_SCALED 0
+#define FMX_EIGEN_OP_GRAM 1
 #define FMX_EIGEN_PLAIN 0   /* FP32 SpMM operands; dense products in FP64 on CUDA cores */
 #define FMX_EIGEN_MIXED 1   /* filter in correction form with BF16 SpMM operands (FP32
                                accumulation), Rayleigh-Ritz SpMM in FP32; CholQR basis
@@ -251,6 +253,12 @@ typedef struct fmx_eigen_options {
 	uint64_t seed;      /* random start block, uniform(-1, 1) (MvRandom) */
 	const float *X0;    /* optional start block on the device (n x block_size), or NULL */
 	int64_t ldx0;
+	int op;             /* FMX_EIGEN_OP_SCALED: diag(s) A diag(s) (A square);
+	                       FMX_EIGEN_OP_GRAM: A^T A on ncols-vectors, through the
+	                       transpose (SVD_Operator, matrix/test/test-eigen.cpp:138-177):
+	                       its eigenpairs are the squared singular values and right
+	                       singular vectors of A; the bounds must enclose
+	                       [0, sigma_max^2] and no row scale is taken */
 } fmx_eigen_options;
 
 typedef struct fmx_eigen_status {
@@ -264,7 +272,7 @@ typedef struct fmx_eigen_status {
 
 /* Defaults as eigen_options() and init(nev) (eigensolver.cpp:82-116): tol 1e-8,
  * max_iters 500, block_size max(2 nev, 16) (at most 64), degree 16, LA, plain,
- * spectrum [-1, 1], seed 1. */
+ * spectrum [-1, 1], seed 1, op FMX_EIGEN_OP_SCALED. */
 void fmx_eigen_default_options(fmx_eigen_options *opts, int nev);
 
 /* Solve; evals and residuals are host arrays of nev, evecs a device array of

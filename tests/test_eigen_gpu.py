@@ -189,3 +189,45 @@ def test_argument_errors(torch_cuda):
     with pytest.raises(FmxError) as e:
         compute_eigen(rect, True, opts)
     assert e.value.code == _lib.FMX_ERR_DIM
+
+
+@pytest.mark.parametrize("precision", ["plain", "mixed"])
+def test_svd_operator_rectangular(torch_cuda, precision):
+    """A^T A of a rectangular weighted matrix through its transpose
+    (SVD_Operator, test-eigen.cpp:138-177): eigenvalues are the squared
+    singular values (scipy svds, FP64), vectors the right singular vectors."""
+    from scipy.sparse.linalg import svds
+    from flashx_b200 import create_2d_matrix
+    from flashx_b200.eigen import SVD_operator
+    rng = np.random.default_rng(21)
+    nr, nc, m = 5000, 3000, 60000
+    src = rng.integers(0, nr, m).astype(np.uint32)
+    dst = rng.integers(0, nc, m).astype(np.uint32)
+    # a planted low-rank part so that the top singular values are separated
+    src = np.concatenate([src, rng.integers(0, 200, 8000).astype(np.uint32)])
+    dst = np.concatenate([dst, rng.integers(0, 150, 8000).astype(np.uint32)])
+    vals = rng.uniform(0.5, 1.5, len(src)).astype(np.float32)
+    mat = create_2d_matrix(src, dst, vals, block_size=(1024, 1024), is_sym=False, nrows=nr, ncols=nc)
+    keep = src != dst                      # the builder drops (i, i) entries (set_remove_self_edge default)
+    A = sp.csr_matrix((vals[keep].astype(np.float64), (src[keep], dst[keep])), shape=(nr, nc))
+    A.sum_duplicates()
+    opts = eigen_options()
+    opts.init(4)
+    opts.which = "LA"
+    opts.tol = TOL
+    opts.precision = precision
+    op = SVD_operator(mat)
+    res = compute_eigen(op, True, opts)
+    assert res.status.converged == 4
+    X = res.vecs.double().cpu().numpy()
+    N = (A.T @ A).tocsr()
+    norm = float(svds(A, k=1, return_singular_vectors=False)[0]) ** 2
+    assert norm <= op.upper * (1 + 1e-6)       # the filter's bound holds
+    # residuals relative to the bound the solver normalises by
+    r = np.linalg.norm(N @ X - X * res.vals, axis=0) / np.linalg.norm(X, axis=0) / op.upper
+    assert r.max() <= 2 * TOL
+    u, sv, vt = svds(A, k=6)
+    order = np.argsort(-sv)
+    sv, vt = sv[order], vt[order]
+    np.testing.assert_allclose(res.vals, sv[:4] ** 2, rtol=1e-6)
+    assert _sin_angle(X, vt[:4].T) <= 1e-4
