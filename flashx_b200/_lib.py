@@ -34,6 +34,7 @@ EIGEN_OP_SCALED, EIGEN_OP_GRAM = 0, 1
 BUILD_DEDUP = 0x1
 BUILD_KEEP_SELF_LOOPS = 0x2
 BUILD_REF_VALUE_LAYOUT = 0x4
+BUILD_TRANSPOSE = 0x8
 
 
 class FmxError(RuntimeError):
@@ -99,6 +100,7 @@ _SIGS = {
     "fmx_dense_gram": (_int, [_int, _vp, _i64, _int, _vp, _i64, _int, _i64, _vp, _vp, _vp, _vp]),
     "fmx_dense_chol_inv": (_int, [_vp, _int, _vp, _vp, _vp]),
     "fmx_dense_sym_eig": (_int, [_vp, _int, _vp, _vp, _vp]),
+    "fmx_matrix_build_device": (_int, [_vp, _vp, _vp, _int, _u64, _u64, _u64, _int, _int, _vp, _P(_vp)]),
     "fmx_eigen_default_options": (None, [_P(eigen_options_t), _int]),
     "fmx_eigen_solve": (_int, [_vp, _vp, _P(eigen_options_t), _vp, _vp, _i64, _vp, _P(eigen_status_t), _vp]),
     "fmx_na_scale": (_int, [_vp, _vp, _vp]),

@@ -1167,6 +1167,43 @@ int fmx_matrix_create(const fmx_image *img, const fmx_image *t_img, int device, 
 	return FMX_OK;
 }
 
+int fmx_matrix_build_device(const uint32_t *src, const uint32_t *dst, const void *vals, int val_type,
+		uint64_t nedges, uint64_t nrows, uint64_t ncols, int flags, int device, void *stream, fmx_matrix **out)
+{
+	if (!out || (nedges && (!src || !dst)) || (val_type != FMX_P_BOOL && nedges && !vals))
+		return set_error(FMX_ERR_INVAL, "null argument");
+	*out = nullptr;
+	if (flags & ~(FMX_BUILD_DEDUP | FMX_BUILD_KEEP_SELF_LOOPS | FMX_BUILD_TRANSPOSE))
+		return set_error(FMX_ERR_INVAL, "flags 0x%x: the device builder takes DEDUP, KEEP_SELF_LOOPS and TRANSPOSE",
+				flags);
+	int ndev = 0;
+	if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return set_error(FMX_ERR_CUDA, "no CUDA device is available");
+	if (device < 0 || device >= ndev) return set_error(FMX_ERR_INVAL, "device %d out of range (%d devices)", device, ndev);
+	int cur = 0;
+	cudaGetDevice(&cur);
+	CUDA_TRY(cudaSetDevice(device));
+	std::unique_ptr<fmx_matrix> m(new (std::nothrow) fmx_matrix);
+	int rc = m ? FMX_OK : set_error(FMX_ERR_OOM, "out of host memory");
+	cudaStream_t st = static_cast<cudaStream_t>(stream);
+	try {
+		host_csr csr;
+		if (!rc) rc = edges_to_csr_device(src, dst, vals, val_type, nedges, nrows, ncols, flags, st, csr);
+		if (!rc) rc = make_part(csr, device, m->a);
+		if (!rc && (flags & FMX_BUILD_TRANSPOSE)) {
+			host_csr t;
+			rc = edges_to_csr_device(dst, src, vals, val_type, nedges, csr.ncols, csr.nrows, flags, st, t);
+			if (!rc) rc = make_part(t, device, m->at);
+		}
+	} catch (const std::bad_alloc &) {
+		rc = set_error(FMX_ERR_OOM, "host allocation failed in the device builder");
+	}
+	cudaSetDevice(cur);
+	if (rc) return rc;
+	m->symmetric = !(flags & FMX_BUILD_TRANSPOSE);
+	*out = m.release();
+	return FMX_OK;
+}
+
 int fmx_matrix_load(const char *mat_idx_path, const char *mat_path, const char *t_mat_idx_path,
 		const char *t_mat_path, int device, fmx_matrix **out)
 {

@@ -207,6 +207,42 @@ class sparse_matrix:
                                   device, C.byref(h)))
         return cls(h.value, device)
 
+    @classmethod
+    def from_device_edges(cls, src, dst, vals=None, nrows=0, ncols=0, dedup=None, remove_self=None,
+                          transpose=False, stream=None):
+        """The matrix straight from an edge list already on a GPU (int32 or
+        uint32-valued CUDA tensors; vals: a float32/float64/int32/int64 CUDA
+        tensor or None): fmx_matrix_build_device sorts and deduplicates on
+        that GPU, with the same result as create_2d_matrix on the host.
+        transpose=True also builds A^T (a directed graph's asymmetric pair)."""
+        import torch
+        if src.shape != dst.shape or not src.is_cuda or src.device != dst.device:
+            raise ValueError("src and dst must be CUDA tensors of one shape on one device")
+        if src.dtype != torch.int32 or dst.dtype != torch.int32:
+            raise ValueError("src and dst must be int32 tensors (ids < 2^31)")
+        src, dst = src.contiguous(), dst.contiguous()
+        prim, vptr = _lib.P_BOOL, None
+        if vals is not None:
+            prim = {torch.float32: _lib.P_FLOAT, torch.float64: _lib.P_DOUBLE, torch.int32: _lib.P_INTEGER,
+                    torch.int64: _lib.P_LONG}.get(vals.dtype)
+            if prim is None or vals.shape != src.shape or vals.device != src.device:
+                raise ValueError("vals must be a float32/float64/int32/int64 CUDA tensor like src")
+            vals = vals.contiguous()
+            vptr = vals.data_ptr()
+        flags = 0
+        if (_dedup if dedup is None else dedup):
+            flags |= _lib.BUILD_DEDUP
+        if not (_remove_self if remove_self is None else remove_self):
+            flags |= _lib.BUILD_KEEP_SELF_LOOPS
+        if transpose:
+            flags |= _lib.BUILD_TRANSPOSE
+        dev = src.device.index
+        st = stream if stream is not None else torch.cuda.current_stream(src.device).cuda_stream
+        h = C.c_void_p()
+        check(lib.fmx_matrix_build_device(src.data_ptr(), dst.data_ptr(), vptr, prim, src.numel(), nrows, ncols,
+                                          flags, dev, st, C.byref(h)))
+        return cls(h.value, dev)
+
     # -- reference accessors --
     def get_num_rows(self):
         return self._nrows

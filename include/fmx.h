@@ -115,6 +115,22 @@ int fmx_image_free(fmx_image *img);
  */
 int fmx_matrix_create(const fmx_image *img, const fmx_image *t_img, int device,
                       fmx_matrix **out);
+/* Build the resident matrix straight from an edge list in the memory of
+ * `device` (src_dev, dst_dev: uint32 ids; vals_dev: nedges values of
+ * val_type, or NULL for FMX_P_BOOL): the sort, deduplication and row
+ * pointers of fm::create_2d_matrix (matrix/fm_utils.cpp:267-433) run on the
+ * GPU, the work schedule on the host, with no .mat image in between.  The
+ * same entries in the same order as fmx_image_build + fmx_matrix_create with
+ * the same flags, so SpMM results are identical.  flags: FMX_BUILD_DEDUP,
+ * FMX_BUILD_KEEP_SELF_LOOPS, FMX_BUILD_TRANSPOSE (also build A^T, the
+ * asymmetric pair create_2d_matrix makes for a directed graph).  nrows /
+ * ncols = 0: the largest id + 1.  Fewer than 2^31 edges.  Synchronises
+ * `stream`. */
+#define FMX_BUILD_TRANSPOSE 0x8
+int fmx_matrix_build_device(const uint32_t *src_dev, const uint32_t *dst_dev,
+                            const void *vals_dev, int val_type, uint64_t nedges,
+                            uint64_t nrows, uint64_t ncols, int flags, int device,
+                            void *stream, fmx_matrix **out);
 /* Convenience: fmx_image_load + fmx_matrix_create (+ free of the images). */
 int fmx_matrix_load(const char *mat_idx_path, const char *mat_path,
                     const char *t_mat_idx_path, const char *t_mat_path,
