@@ -94,6 +94,28 @@ int edges_to_csr_device(const uint32_t *src, const uint32_t *dst, const void *va
 
 int default_threads();
 
+// ---- fused PageRank iteration ----------------------------------------------
+// The update of fm::alg::PageRank (PageRank.cpp:110-123) applied where the
+// SpMV on A^T closes a row: p2 = out * d + teleport; converged += |pr1 - p2|
+// < eps; pr = p2; in_next = p2 / deg; pr1 = in_next * deg.  state[0] counts
+// this iteration's converged vertices, state[1] is the done flag (set once
+// every vertex converged or the iteration cap is reached; the kernels of
+// later iterations then return at once), state[2] the iterations run.
+struct pr_epi {
+	const float *deg;
+	const uint32_t *heavy_mask;    // bit per row summed by the fixup (chunked rows)
+	float *pr, *pr1, *in_next;
+	unsigned long long *state;
+	float damping, teleport, eps;
+	unsigned long long n, max_iters;
+};
+// One iteration on the transpose part of `mt`: SpMV of `in` with the update
+// fused, then the iteration's convergence test on the device.
+int pagerank_iteration(const fmx_matrix *mt, const float *in, const pr_epi &e, cudaStream_t st);
+// Set heavy_mask (ceil(nrows / 32) words, zeroed by the caller) from mt's
+// chunked rows.
+int pagerank_heavy_mask(const fmx_matrix *mt, uint32_t *mask, cudaStream_t st);
+
 } // namespace fmx
 
 struct fmx_image {

@@ -12,9 +12,15 @@
 //     converged = #{ |pr1 - pr2| < 0.001 / n }        (:94, :118-123)
 //     pr  = pr2
 //
-// One iteration is the SpMV (fmx_spmm on the transpose, k = 1) and one fused
-// kernel that applies the damping, counts the converged vertices and writes
-// the next iteration's input (pr / deg and its in * deg reconstruction).
+// One iteration is one pass: the SpMV on the transpose (k = 1) applies the
+// damping, counts the converged vertices and writes the next input where it
+// closes each row (rows summed in chunks get the same update in the fixup
+// kernel), and a one-thread kernel runs the loop test on the device.  The
+// input is double-buffered (other rows still gather this iteration's input
+// while the next one is written).  Iterations are queued in batches with one
+// host read of the loop state per batch; an iteration queued after the loop
+// ended returns at once, so the result and the count match a loop that
+// tests on the host after every iteration.
 #include "fmx_internal.h"
 
 #include <cuda_runtime.h>
@@ -26,6 +32,7 @@ namespace fmx {
 namespace pagerank {
 
 constexpr int kThreads = 256;
+constexpr uint64_t kBatch = 8;          // iterations queued per host read of the loop state
 
 #define PCUDA_TRY(call)                                                         \
 	do {                                                                        \
@@ -56,34 +63,6 @@ __global__ void init_kernel(float *__restrict__ deg, float *__restrict__ pr, flo
 		const float x = __fdiv_rn(p0, d);
 		in[i] = x;
 		pr1[i] = __fmul_rn(x, d);
-	}
-}
-
-// pr2 = out * d + t; count |pr1 - pr2| < eps; pr = pr2; in = pr2 / deg;
-// pr1 = in * deg (the next iteration's reconstruction)
-__global__ void __launch_bounds__(kThreads) update_kernel(const float *__restrict__ out, const float *__restrict__ deg,
-		float *__restrict__ pr, float *__restrict__ in, float *__restrict__ pr1, int64_t n, float damping,
-		float teleport, float eps, unsigned long long *__restrict__ converged)
-{
-	__shared__ unsigned int red[kThreads / 32];
-	unsigned int cnt = 0;
-	for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
-		const float p2 = __fadd_rn(__fmul_rn(out[i], damping), teleport);
-		const float diff = fabsf(__fsub_rn(pr1[i], p2));
-		cnt += diff < eps;
-		pr[i] = p2;
-		const float d = deg[i];
-		const float x = __fdiv_rn(p2, d);
-		in[i] = x;
-		pr1[i] = __fmul_rn(x, d);
-	}
-	for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, o);
-	if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = cnt;
-	__syncthreads();
-	if (threadIdx.x == 0) {
-		unsigned long long s = 0;
-		for (int w = 0; w < kThreads / 32; w++) s += red[w];
-		atomicAdd(converged, s);
 	}
 }
 
@@ -125,43 +104,55 @@ int fmx_pagerank(const fmx_matrix *m, uint64_t max_iters, float damping, float *
 	} g{mt, static_cast<cudaStream_t>(stream), {}};
 	cudaStream_t st = g.st;
 	const int64_t n = int64_t(nr);
-	float *deg, *in, *pr1, *out, *ones;
-	unsigned long long *conv;
-	for (float **b : {&deg, &in, &pr1, &out, &ones}) {
-		void *q = nullptr;
-		cudaError_t e = cudaMallocAsync(&q, size_t(std::max<int64_t>(n, 1)) * sizeof(float), st);
+	float *deg, *in0, *in1, *pr1;
+	uint32_t *mask;
+	unsigned long long *state;
+	auto alloc = [&](void **q, size_t bytes) -> int {
+		cudaError_t e = cudaMallocAsync(q, std::max<size_t>(bytes, 16), st);
 		if (e != cudaSuccess) return set_error(FMX_ERR_OOM, "PageRank vectors: %s", cudaGetErrorString(e));
-		g.bufs.push_back(q);
-		*b = static_cast<float *>(q);
-	}
-	{
-		void *q = nullptr;
-		PCUDA_TRY(cudaMallocAsync(&q, sizeof(unsigned long long), st));
-		g.bufs.push_back(q);
-		conv = static_cast<unsigned long long *>(q);
-	}
-	// the convergence count comes back through one pinned word per host thread
-	static thread_local unsigned long long *hconv = nullptr;
-	if (!hconv) PCUDA_TRY(cudaMallocHost(&hconv, sizeof(unsigned long long)));
+		g.bufs.push_back(*q);
+		return FMX_OK;
+	};
+	const size_t mask_words = size_t((n + 31) / 32);
+	for (float **b : {&deg, &in0, &in1, &pr1}) P_TRY(alloc(reinterpret_cast<void **>(b), size_t(n) * sizeof(float)));
+	P_TRY(alloc(reinterpret_cast<void **>(&mask), mask_words * sizeof(uint32_t)));
+	P_TRY(alloc(reinterpret_cast<void **>(&state), 3 * sizeof(unsigned long long)));
+	// the loop state comes back through three pinned words per host thread
+	static thread_local unsigned long long *hstate = nullptr;
+	if (!hstate) PCUDA_TRY(cudaMallocHost(&hstate, 3 * sizeof(unsigned long long)));
 	const unsigned gb = grid_for(n);
-	fill_kernel<<<gb, kThreads, 0, st>>>(ones, n, 1.0f);
+	fill_kernel<<<gb, kThreads, 0, st>>>(in1, n, 1.0f);
 	PCUDA_TRY(cudaGetLastError());
-	P_TRY(fmx_spmm(m, FMX_F32, ones, 1, FMX_F32, deg, 1, 1, nullptr, nullptr, st));
+	P_TRY(fmx_spmm(m, FMX_F32, in1, 1, FMX_F32, deg, 1, 1, nullptr, nullptr, st));
 	const float p0 = float(1.0 / double(n));
-	const float eps = float(0.001 / double(n));
-	const float teleport = float((1.0 - double(damping)) / double(n));
-	init_kernel<<<gb, kThreads, 0, st>>>(deg, pr, in, pr1, n, p0);
+	pr_epi e{};
+	e.deg = deg;
+	e.heavy_mask = mask;
+	e.pr = pr;
+	e.pr1 = pr1;
+	e.state = state;
+	e.damping = damping;
+	e.teleport = float((1.0 - double(damping)) / double(n));
+	e.eps = float(0.001 / double(n));
+	e.n = uint64_t(n);
+	e.max_iters = max_iters;
+	init_kernel<<<gb, kThreads, 0, st>>>(deg, pr, in0, pr1, n, p0);
 	PCUDA_TRY(cudaGetLastError());
-	uint64_t it = 0, converged = 0;
-	while (converged < uint64_t(n) && it < max_iters) {
-		PCUDA_TRY(cudaMemsetAsync(conv, 0, sizeof(unsigned long long), st));
-		P_TRY(fmx_spmm(mt, FMX_F32, in, 1, FMX_F32, out, 1, 1, nullptr, nullptr, st));
-		update_kernel<<<gb, kThreads, 0, st>>>(out, deg, pr, in, pr1, n, damping, teleport, eps, conv);
-		PCUDA_TRY(cudaGetLastError());
-		PCUDA_TRY(cudaMemcpyAsync(hconv, conv, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+	PCUDA_TRY(cudaMemsetAsync(mask, 0, mask_words * sizeof(uint32_t), st));
+	PCUDA_TRY(cudaMemsetAsync(state, 0, 3 * sizeof(unsigned long long), st));
+	P_TRY(pagerank_heavy_mask(mt, mask, st));
+	uint64_t it = 0, queued = 0;
+	while (n > 0 && queued < max_iters) {
+		const uint64_t batch = std::min<uint64_t>(kBatch, max_iters - queued);
+		for (uint64_t b = 0; b < batch; b++, queued++) {
+			const float *in = (queued & 1) ? in1 : in0;
+			e.in_next = (queued & 1) ? in0 : in1;
+			P_TRY(pagerank_iteration(mt, in, e, st));
+		}
+		PCUDA_TRY(cudaMemcpyAsync(hstate, state, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
 		PCUDA_TRY(cudaStreamSynchronize(st));
-		converged = *hconv;
-		it++;
+		it = hstate[2];
+		if (hstate[1]) break;
 	}
 	if (iters) *iters = it;
 	return FMX_OK;

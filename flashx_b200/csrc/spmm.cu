@@ -459,9 +459,24 @@ __device__ __forceinline__ void ld_w(const void *val, uint32_t step, A (&w)[U])
 // row when its end flag passes; chunks of longer rows leave their sum in
 // partial[slot].  Hot entries read the packed rows (which already carry
 // s_in); the others read X and, with SCALE_IN, s_in.
-template <class XT, class YT, class A, class WT, int VEC, int NV, int U, bool SCALE_IN, bool SCALE_OUT>
+// The PageRank update at a row close (EPI): rows of the fixup's heavy list
+// are left to the fixup.
+__device__ __forceinline__ void pr_update(const pr_epi &e, int64_t row, float out, unsigned &cnt)
+{
+	const float p2 = __fadd_rn(__fmul_rn(out, e.damping), e.teleport);
+	const float diff = fabsf(__fsub_rn(e.pr1[row], p2));
+	cnt += diff < e.eps;
+	e.pr[row] = p2;
+	const float d = e.deg[row];
+	const float x = __fdiv_rn(p2, d);
+	e.in_next[row] = x;
+	e.pr1[row] = __fmul_rn(x, d);
+}
+
+template <class XT, class YT, class A, class WT, int VEC, int NV, int U, bool SCALE_IN, bool SCALE_OUT,
+		bool EPI = false>
 __device__ __forceinline__ void run_range(const spmm_args &a, const range_t rg, int colbase,
-		uint64_t pol_hot, uint64_t pol_cold)
+		uint64_t pol_hot, uint64_t pol_cold, const pr_epi &e, unsigned &cnt)
 {
 	const XT *X = static_cast<const XT *>(a.X);
 	const XT *H = static_cast<const XT *>(a.xhot);
@@ -516,7 +531,11 @@ __device__ __forceinline__ void run_range(const spmm_args &a, const range_t rg, 
 					else acc.template add<XT, 0>(v, x[u][v], A(1), A(1));
 				}
 			const bool end = runs && ((ends >> u) & 1u);
-			if constexpr (NV == 1) {
+			if constexpr (EPI) {
+				static_assert(NV == 1 && VEC == 1 && std::is_same<A, float>::value, "PageRank: k = 1, FP32");
+				if (end && !((__ldg(e.heavy_mask + (row >> 5)) >> (row & 31)) & 1u))
+					pr_update(e, int64_t(row), acc.get(0, 0), cnt);
+			} else if constexpr (NV == 1) {
 				// branch-free row close: predicated store, select-reset
 				YT *Yp = static_cast<YT *>(a.Y) + int64_t(row) * a.ldy + colbase;
 				A so = A(1);
@@ -546,10 +565,14 @@ __device__ __forceinline__ void run_range(const spmm_args &a, const range_t rg, 
 	}
 }
 
-template <class XT, class YT, class A, class WT, int VEC, int NV, int U, bool SCALE_IN, bool SCALE_OUT>
+template <class XT, class YT, class A, class WT, int VEC, int NV, int U, bool SCALE_IN, bool SCALE_OUT,
+		bool EPI = false>
 __global__ void __launch_bounds__(kThreads, sizeof(XT) == 2 ? FMX_SPMM_MIN_BLOCKS_2B : FMX_SPMM_MIN_BLOCKS)
-spmm_kernel(const spmm_args a)
+spmm_kernel(const spmm_args a, const pr_epi e)
 {
+	if constexpr (EPI) {
+		if (e.state[1]) return;           // converged in an earlier iteration
+	}
 	const int lane = threadIdx.x & 31;
 	const uint32_t gw = (blockIdx.x * kThreads + threadIdx.x) >> 5;
 	const uint32_t nw = (gridDim.x * kThreads) >> 5;
@@ -560,8 +583,115 @@ spmm_kernel(const spmm_args a)
 	const uint32_t gg = gw * uint32_t(R) + uint32_t(grp);
 	const uint32_t ng = nw * uint32_t(R);
 	const uint64_t pol_hot = policy_evict_last(), pol_cold = policy_evict_first();
+	unsigned cnt = 0;
 	for (uint32_t r = gg; r < a.n_ranges; r += ng)
-		run_range<XT, YT, A, WT, VEC, NV, U, SCALE_IN, SCALE_OUT>(a, a.ranges[r], colbase, pol_hot, pol_cold);
+		run_range<XT, YT, A, WT, VEC, NV, U, SCALE_IN, SCALE_OUT, EPI>(a, a.ranges[r], colbase, pol_hot, pol_cold,
+				e, cnt);
+	if constexpr (EPI) {
+		// G = 1: every lane of the warp is a row group and reaches this point
+		cnt = __reduce_add_sync(0xffffffffu, cnt);
+		if (lane == 0 && cnt) atomicAdd(e.state, (unsigned long long)cnt);
+	}
+}
+
+// k = 1 (SpMV): a warp per range.  The 32 lanes load the range's column ids
+// (coalesced) and gather its X values into shared memory, one entry each;
+// then each lane sums whole rows of the range from shared memory in entry
+// order, with one running sum per row and every add rounded, which is the
+// lane-group kernel's arithmetic: rows of up to 256 entries come out
+// identical.  A chunk of a longer row is added up by the whole warp (each
+// lane its own entries, then a fixed xor tree) into its partial slot.  (The lane-group
+// kernel at k = 1 gives each lane a whole range and waits on one step of 4
+// gathers at a time.)
+constexpr int kSpmvMax = 512;            // most entries of one range
+static_assert(((kRange - 1 + kExactMax + kStep - 1) / kStep) * kStep <= uint32_t(kSpmvMax) &&
+		kChunk <= uint32_t(kSpmvMax), "a range fits the SpMV kernel's staging");
+
+template <class T, class WT, bool EPI>
+__global__ void __launch_bounds__(kThreads) spmv_kernel(const spmm_args a, const pr_epi e)
+{
+	if constexpr (EPI) {
+		if (e.state[1]) return;           // converged in an earlier iteration
+	}
+	constexpr int kWarps = kThreads / 32;
+	constexpr int J = kSpmvMax / 32;
+	constexpr bool kBinary = std::is_void<WT>::value;
+	__shared__ T sval[kWarps][kSpmvMax];
+	__shared__ uint16_t send[kWarps][kSpmvMax];
+	const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+	const uint32_t gw = (blockIdx.x * kThreads + threadIdx.x) >> 5;
+	const uint32_t nw = (gridDim.x * kThreads) >> 5;
+	const T *X = static_cast<const T *>(a.X);
+	const T *H = static_cast<const T *>(a.xhot);
+	const uint64_t pol_hot = policy_evict_last(), pol_cold = policy_evict_first();
+	unsigned cnt = 0;
+	for (uint32_t r = gw; r < a.n_ranges; r += nw) {
+		const range_t rg = a.ranges[r];
+		const bool runs = rg.slot == kNoSlot;
+		uint32_t raw[J];
+#pragma unroll
+		for (int j = 0; j < J; j++) {
+			const uint32_t i = uint32_t(j * 32 + lane);
+			raw[j] = i < rg.len ? __ldcs(a.col + rg.e0 + i) : 0u;
+		}
+		T t[J];
+#pragma unroll
+		for (int j = 0; j < J; j++) {
+			const uint32_t i = uint32_t(j * 32 + lane);
+			t[j] = T(0);
+			if (i < rg.len) {
+				const uint32_t c = raw[j] & kIdxMask;
+				const bool hot = raw[j] & kHot;
+				t[j] = ld_x_hint<T, 1>((hot ? H : X) + int64_t(c) * (hot ? int64_t(1) : a.ldx),
+						hot ? pol_hot : pol_cold).v[0];
+			}
+		}
+		if constexpr (!kBinary) {
+#pragma unroll
+			for (int j = 0; j < J; j++) {
+				const uint32_t i = uint32_t(j * 32 + lane);
+				if (i < rg.len) t[j] = acc_mul(t[j], T(__ldcs(static_cast<const WT *>(a.val) + rg.e0 + i)));
+			}
+		}
+		// stage the products and the row ends (entry index of each row's last entry)
+		int nrow = 0;
+#pragma unroll
+		for (int j = 0; j < J; j++) {
+			const uint32_t i = uint32_t(j * 32 + lane);
+			const bool is_end = runs && i < rg.len && (raw[j] >> 31);
+			const uint32_t b = __ballot_sync(0xffffffffu, is_end);
+			if (is_end) send[wib][nrow + __popc(b & ((1u << lane) - 1u))] = uint16_t(i);
+			nrow += __popc(b);
+			sval[wib][i] = t[j];
+		}
+		__syncwarp();
+		if (runs) {
+			for (int q = lane; q < nrow; q += 32) {
+				const int b0 = q ? int(send[wib][q - 1]) + 1 : 0, b1 = send[wib][q];
+				T acc = T(0);
+				for (int i = b0; i <= b1; i++) acc = acc_add(acc, sval[wib][i]);
+				const uint32_t row = rg.row0 + uint32_t(q);
+				if constexpr (EPI) {
+					if (!((__ldg(e.heavy_mask + (row >> 5)) >> (row & 31)) & 1u)) pr_update(e, int64_t(row), acc, cnt);
+				} else {
+					static_cast<T *>(a.Y)[int64_t(row) * a.ldy] = acc;
+				}
+			}
+		} else {
+			// a chunk: each lane adds its entries (j order), then a fixed xor tree
+			T acc = T(0);
+#pragma unroll
+			for (int j = 0; j < J; j++) acc = acc_add(acc, t[j]);
+#pragma unroll
+			for (int o = 16; o > 0; o >>= 1) acc = acc_add(acc, __shfl_xor_sync(0xffffffffu, acc, o));
+			if (lane == 0) static_cast<T *>(a.partial)[int64_t(rg.slot) * kPartialStride] = acc;
+		}
+		__syncwarp();
+	}
+	if constexpr (EPI) {
+		cnt = __reduce_add_sync(0xffffffffu, cnt);
+		if (lane == 0 && cnt) atomicAdd(e.state, (unsigned long long)cnt);
+	}
 }
 
 // Pack the hot columns' X rows of this panel behind a zero row:
@@ -595,10 +725,13 @@ __global__ void pack_hot_kernel(const int32_t *hot_col, uint32_t n_hot, const XT
 // kLongChunks chunks) gets a warp with P = 32 / L; the rest go 32 / (2 L)
 // rows to a warp with P = 2 (one row and P = 1 when L = 32).  Deterministic,
 // with many loads in flight.
-template <class YT, class A, bool SCALE_OUT>
+template <class YT, class A, bool SCALE_OUT, bool EPI = false>
 __global__ void spmm_fixup_kernel(const heavy_row *heavy, uint32_t n_heavy, uint32_t n_long, const A *partial,
-		YT *Y, int64_t ldy, int k, const A *s_out, int L)
+		YT *Y, int64_t ldy, int k, const A *s_out, int L, const pr_epi e)
 {
+	if constexpr (EPI) {
+		if (e.state[1]) return;
+	}
 	constexpr bool kVec4 = std::is_same<A, float>::value;
 	const bool vec = kVec4 && (k % 4) == 0;
 	const int units = vec ? k / 4 : k;
@@ -655,6 +788,14 @@ __global__ void spmm_fixup_kernel(const heavy_row *heavy, uint32_t n_heavy, uint
 		for (int o = L; o < lanes; o <<= 1)
 #pragma unroll
 			for (int i = 0; i < 4; i++) t[i] = acc_add(t[i], __shfl_xor_sync(0xffffffffu, t[i], o));
+		if constexpr (EPI) {
+			if (mine && part == 0) {
+				unsigned c = 0;
+				pr_update(e, h.row, t[0], c);
+				if (c) atomicAdd(e.state, 1ull);
+			}
+			continue;
+		}
 		if (mine && part == 0) {
 			A so = A(1);
 			if constexpr (SCALE_OUT) so = s_out[h.row];
@@ -668,9 +809,9 @@ __global__ void spmm_fixup_kernel(const heavy_row *heavy, uint32_t n_heavy, uint
 	}
 }
 
-template <class YT, class A, bool SCALE_OUT>
+template <class YT, class A, bool SCALE_OUT, bool EPI = false>
 static int launch_fixup(const gpu_part &p, const A *partial, YT *Y, int64_t ldy, int k, const A *s_out,
-		cudaStream_t st)
+		cudaStream_t st, const pr_epi &e = pr_epi{})
 {
 	if (!p.n_heavy) return FMX_OK;
 	const bool vec = std::is_same<A, float>::value && (k % 4) == 0;
@@ -681,8 +822,8 @@ static int launch_fixup(const gpu_part &p, const A *partial, YT *Y, int64_t ldy,
 	const uint64_t per_warp = uint64_t(32 / (L * (L < 32 ? 2 : 1)));    // short rows per warp
 	const uint64_t warps = p.n_long_heavy + (n_short + per_warp - 1) / per_warp;
 	const unsigned fb = unsigned((warps * 32 + 255) / 256);
-	spmm_fixup_kernel<YT, A, SCALE_OUT><<<fb, 256, 0, st>>>(p.heavy, p.n_heavy, p.n_long_heavy, partial, Y, ldy,
-			k, s_out, L);
+	spmm_fixup_kernel<YT, A, SCALE_OUT, EPI><<<fb, 256, 0, st>>>(p.heavy, p.n_heavy, p.n_long_heavy, partial, Y,
+			ldy, k, s_out, L, e);
 	CUDA_TRY(cudaGetLastError());
 	return FMX_OK;
 }
@@ -917,7 +1058,7 @@ static int launch_one(const gpu_part &p, const spmm_args &a, cudaStream_t st)
 	static unsigned blocks[64] = {0};
 	unsigned &b = blocks[p.device & 63];
 	if (!b) b = persistent_blocks(kern, p.device);
-	kern<<<b, kThreads, 0, st>>>(a);
+	kern<<<b, kThreads, 0, st>>>(a, pr_epi{});
 	CUDA_TRY(cudaGetLastError());
 	return FMX_OK;
 }
@@ -951,10 +1092,40 @@ static int launch_t(const gpu_part &p, spmm_args a, bool sin, bool sout, cudaStr
 static bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
 
 // Run one orientation over all column panels (kPanelBytes of X row each).
+// k = 1 without row scales: pack, the warp-per-range SpMV, fixup.
+template <class T, class WT, bool EPI>
+static int run_spmv(const gpu_part &p, const T *X, int64_t ldx, T *Y, int64_t ldy, cudaStream_t st,
+		const pr_epi &e = pr_epi{})
+{
+	spmm_args a{};
+	a.col = p.col; a.val = p.val; a.ranges = p.ranges;
+	a.X = X; a.xhot = p.xhot; a.hot_ld = 1;
+	a.Y = Y;
+	a.partial = p.partial;
+	a.ldx = ldx; a.ldy = ldy; a.k = 1;
+	a.G = 1; a.R = 32; a.nv = 1;
+	a.n_ranges = p.n_ranges;
+	const unsigned pb = unsigned(std::min<uint64_t>((uint64_t(p.n_hot) + 256) / 256, 148ull * 16));
+	pack_hot_kernel<T, T, false><<<pb, 256, 0, st>>>(p.hot_col, p.n_hot, X, ldx, 1, static_cast<T *>(p.xhot), 1,
+			nullptr);
+	CUDA_TRY(cudaGetLastError());
+	auto kern = spmv_kernel<T, WT, EPI>;
+	static unsigned blocks[64] = {0};
+	unsigned &b = blocks[p.device & 63];
+	if (!b) b = persistent_blocks(kern, p.device);
+	kern<<<b, kThreads, 0, st>>>(a, e);
+	CUDA_TRY(cudaGetLastError());
+	return launch_fixup<T, T, false, EPI>(p, static_cast<const T *>(p.partial), Y, ldy, 1, nullptr, st, e);
+}
+
 template <class XT, class YT, class A, class WT>
 static int run_typed(const gpu_part &p, const void *X, int64_t ldx, void *Y, int64_t ldy, int64_t k,
 		const void *sin, const void *sout, cudaStream_t st)
 {
+	if constexpr (std::is_same<XT, A>::value && std::is_same<YT, A>::value && std::is_floating_point<A>::value) {
+		if (k == 1 && !sin && !sout)
+			return run_spmv<A, WT, false>(p, static_cast<const A *>(X), ldx, static_cast<A *>(Y), ldy, st);
+	}
 	constexpr int VEC = int(16 / sizeof(XT));
 	constexpr int kPanel = kPanelBytes / int(sizeof(XT));
 	// 16-byte vectors along k when every X and Y row starts 16-byte aligned
@@ -1040,6 +1211,56 @@ int spmm_part(const gpu_part &p, int xt, const void *X, int64_t ldx, int yt, voi
 			"(input and output matrices need the same type, sparse_matrix.cpp:754-758)", xt, yt);
 	if (cur != p.device) cudaSetDevice(cur);
 	return rc;
+}
+
+// ---------------------------------------------------------------------------
+// Fused PageRank iteration (SpMV on A^T with the update at each row close)
+// ---------------------------------------------------------------------------
+
+// The iteration's convergence test (PageRank.cpp:96,124-129): one thread.
+__global__ void pr_finish_kernel(unsigned long long *state, unsigned long long n, unsigned long long max_iters)
+{
+	if (threadIdx.x == 0 && !state[1]) {
+		const unsigned long long it = ++state[2];
+		if (state[0] >= n || it >= max_iters) state[1] = 1;
+		state[0] = 0;
+	}
+}
+
+__global__ void heavy_mask_kernel(const heavy_row *heavy, uint32_t n_heavy, uint32_t *mask)
+{
+	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_heavy; i += gridDim.x * blockDim.x) {
+		const uint32_t r = uint32_t(heavy[i].row);
+		atomicOr(mask + (r >> 5), 1u << (r & 31));
+	}
+}
+
+int pagerank_heavy_mask(const fmx_matrix *mt, uint32_t *mask, cudaStream_t st)
+{
+	const gpu_part &p = *mt->a;
+	if (!p.n_heavy) return FMX_OK;
+	heavy_mask_kernel<<<unsigned(std::min<uint32_t>((p.n_heavy + 255) / 256, 1024)), 256, 0, st>>>(p.heavy,
+			p.n_heavy, mask);
+	CUDA_TRY(cudaGetLastError());
+	return FMX_OK;
+}
+
+template <class WT>
+static int pr_iteration_typed(const gpu_part &p, const float *in, const pr_epi &e, cudaStream_t st)
+{
+	// the update writes pr, pr1 and the next input instead of Y
+	if (int rc = run_spmv<float, WT, true>(p, in, 1, nullptr, 1, st, e)) return rc;
+	pr_finish_kernel<<<1, 32, 0, st>>>(e.state, e.n, e.max_iters);
+	CUDA_TRY(cudaGetLastError());
+	return FMX_OK;
+}
+
+int pagerank_iteration(const fmx_matrix *mt, const float *in, const pr_epi &e, cudaStream_t st)
+{
+	const gpu_part &p = *mt->a;
+	if (p.prim == FMX_P_BOOL) return pr_iteration_typed<void>(p, in, e, st);
+	if (p.prim == FMX_P_FLOAT) return pr_iteration_typed<float>(p, in, e, st);
+	return set_error(FMX_ERR_TYPE, "PageRank: binary or float-weighted matrices");
 }
 
 // ---------------------------------------------------------------------------

@@ -65,3 +65,46 @@ def test_pagerank_errors(torch_cuda):
     with pytest.raises(FmxError) as e:
         PageRank(rect, 10, 0.85)
     assert e.value.code == _lib.FMX_ERR_DIM
+
+
+def test_pagerank_fused_matches_stepwise_loop(torch_cuda):
+    """The fused iteration (update applied where the SpMV closes a row, and
+    in the fixup for chunked hub rows) against a host-driven loop of plain
+    SpMVs on the transpose with the update in float32 numpy (one rounding per
+    operation, as PageRank.cpp:100-123): bit-identical at R-MAT scale 16,
+    whose hub rows go through the fixup, for an iteration cap below, at and
+    above the point of convergence."""
+    torch = torch_cuda
+    from flashx_b200 import set_deduplicate
+    n = 1 << 16
+    src, dst = rmat_edges(16, seed=2)
+    set_deduplicate(True)
+    try:
+        m = create_2d_matrix(src, dst, None, block_size=(16384, 16384), is_sym=False, nrows=n, ncols=n)
+    finally:
+        set_deduplicate(False)
+    mt = m.transpose()
+    assert mt.schedule()[2] > 0                   # heavy rows take the fixup path
+    d = np.float32(0.85)
+    deg = m.multiply(torch.ones((n, 1), device="cuda")).cpu().numpy()[:, 0]
+    deg = np.maximum(deg, np.float32(1))
+    tele = np.float32((1.0 - float(d)) / n)     # (1 - d) / n in double from the float d
+    eps = np.float32(0.001 / n)
+    pr = np.full(n, np.float32(1.0 / n), dtype=np.float32)
+    x = pr / deg
+    pr1 = x * deg
+    ref_iters, ref = [], []
+    it, conv = 0, 0
+    while conv < n and it < 60:
+        out = mt.multiply(torch.from_numpy(x).cuda().reshape(n, 1)).cpu().numpy()[:, 0]
+        p2 = out * d + tele
+        conv = int(np.count_nonzero(np.abs(pr1 - p2) < eps))
+        pr = p2
+        x = p2 / deg
+        pr1 = x * deg
+        it += 1
+        ref.append(pr.copy())
+    for cap in (3, 17, 60):
+        got, git = PageRank(m, cap, 0.85)
+        assert git == min(cap, it)
+        assert np.array_equal(got.cpu().numpy(), ref[git - 1])

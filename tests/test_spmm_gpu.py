@@ -203,6 +203,40 @@ def test_rmat_s18_parity(torch_cuda):
             np.testing.assert_allclose(Y, R, rtol=RTOL, atol=RTOL * np.abs(R).max())
 
 
+@pytest.mark.parametrize("dtype", ["float32", "float64"])
+def test_spmv_kernel_matches_lane_group_kernel(torch_cuda, dtype):
+    """k = 1 without row scales runs the warp-per-range SpMV kernel; with row
+    scales of exactly 1 (x * 1 and y * 1 are exact) it runs the lane-group
+    kernel.  Rows of up to EXACT_ROW_MAX entries have the same arithmetic in
+    both and must agree bit for bit; hub rows (chunks added up in another
+    association) within RTOL."""
+    torch = torch_cuda
+    tdt = getattr(torch, dtype)
+    n = 1 << 17
+    src, dst = rmat_edges(17, seed=4)
+    rng = np.random.default_rng(1)
+    ones = torch.ones(n, device="cuda", dtype=tdt)
+    for weighted in (False, True):
+        vals = rng.uniform(0.0, 1.0, len(src)).astype(np.float32) if weighted else None
+        m = sparse_matrix.create(matrix_image.build(src, dst, vals, nrows=n, ncols=n, block_size=(16384, 16384),
+                                                    dedup=True), None)
+        assert m.schedule()[2] > 0
+        light = torch.from_numpy(np.bincount(src[src != dst].astype(np.int64), minlength=n) <= _lib.EXACT_ROW_MAX)
+        X = torch.randn((n, 1), device="cuda", dtype=tdt)
+        Y1 = m.multiply(X)
+        Ys = torch.empty_like(Y1)
+        assert m.multiply(X, Ys, row_scale_in=ones, row_scale_out=ones)
+        y1, ys = Y1.cpu()[:, 0], Ys.cpu()[:, 0]
+        assert torch.equal(y1[light], ys[light]) and not bool(light.all())
+        torch.testing.assert_close(y1, ys, rtol=RTOL, atol=RTOL * float(ys.abs().max()))
+        # a strided single column (ldx = ldy = 3)
+        X3 = torch.zeros((n, 3), device="cuda", dtype=tdt)
+        X3[:, :1] = X
+        Y3 = torch.full((n, 3), 7.0, device="cuda", dtype=tdt)
+        assert m.multiply(X3[:, :1], Y3[:, :1])
+        assert torch.equal(Y3[:, :1], Y1) and bool((Y3[:, 1:] == 7).all())
+
+
 def test_host_buffers_e2e(torch_cuda):
     src, dst = _graph(5000, 40000, 21)
     idx, mat = oracle.build_image(src, dst, None, block=(1024, 1024), dedup=True)
