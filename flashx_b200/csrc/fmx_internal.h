@@ -94,6 +94,9 @@ int edges_to_csr_device(const uint32_t *src, const uint32_t *dst, const void *va
 
 int default_threads();
 
+// A matrix from host CSR (and its transpose, or null for a symmetric one).
+int matrix_from_csr(const host_csr &a, const host_csr *at, int device, fmx_matrix **out);
+
 // ---- fused PageRank iteration ----------------------------------------------
 // The update of fm::alg::PageRank (PageRank.cpp:110-123) applied where the
 // SpMV on A^T closes a row: p2 = out * d + teleport; converged += |pr1 - p2|

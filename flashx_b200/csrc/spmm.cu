@@ -1349,6 +1349,23 @@ __global__ void rmat_kernel(rmat_params p, uint64_t n, uint32_t *src, uint32_t *
 	}
 }
 
+int matrix_from_csr(const host_csr &a, const host_csr *at, int device, fmx_matrix **out)
+{
+	*out = nullptr;
+	int ndev = 0;
+	if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+		return set_error(FMX_ERR_CUDA, "no CUDA device is available");
+	if (device < 0 || device >= ndev) return set_error(FMX_ERR_INVAL, "device %d out of range (%d devices)", device, ndev);
+	std::unique_ptr<fmx_matrix> m(new (std::nothrow) fmx_matrix);
+	if (!m) return set_error(FMX_ERR_OOM, "out of host memory");
+	if (int rc = make_part(a, device, m->a)) return rc;
+	if (at)
+		if (int rc = make_part(*at, device, m->at)) return rc;
+	m->symmetric = at == nullptr;
+	*out = m.release();
+	return FMX_OK;
+}
+
 } // namespace fmx
 
 using namespace fmx;

@@ -135,6 +135,22 @@ int fmx_matrix_build_device(const uint32_t *src_dev, const uint32_t *dst_dev,
 int fmx_matrix_load(const char *mat_idx_path, const char *mat_path,
                     const char *t_mat_idx_path, const char *t_mat_path,
                     int device, fmx_matrix **out);
+/* The FlashGraph 1D format: fg::create_sparse_matrix(FG_graph::ptr,
+ * entry_type) (flash-graph/fg_sparse_matrix.cpp:577-590) over a graph image
+ * (the adjacency file FG_graph::create reads: graph_header page, then one
+ * ext_mem_undirected_vertex record per vertex, flash-graph/vertex.h:444-562;
+ * a directed graph's in-edge records, then its out-edge records).  Row i is
+ * vertex i's out-edge list (A), its in-edge list for the transpose; an
+ * undirected graph gives a symmetric matrix.  Every stored neighbor counts,
+ * in record order (duplicates and self-loops included), which is the order
+ * fg_row_spmm_task::run_on_row sums in (fg_sparse_matrix.cpp:83-106).
+ * val_type: FMX_P_BOOL for a graph without edge data, else the edge data's
+ * type, whose size must equal the header's edge_data_size (the reference's
+ * assertion, :476-478,551-553).  The vertex index file is not needed: the
+ * records are walked in order.  Time-series graphs: FMX_ERR_UNSUPPORTED. */
+int fmx_matrix_from_fg(const void *adj, size_t adj_len, int val_type, int device,
+                       fmx_matrix **out);
+int fmx_matrix_load_fg(const char *adj_path, int val_type, int device, fmx_matrix **out);
 int fmx_matrix_info(const fmx_matrix *m, uint64_t *nrows, uint64_t *ncols,
                     uint64_t *nnz, int *prim_type, int *symmetric);
 /* Device bytes held by the matrix (tiles, schedule, scratch). */

@@ -18,6 +18,11 @@
  *   - work distribution    matrix/matrix_io.cpp:163-236 (b2d_io_generator),
  *                          libsafs/in_mem_io.cpp:488-512 (per-task memcpy)
  *   - PageRank             matrix/libmatrix-algs/PageRank.cpp:31-133
+ *   - the FlashGraph 1D format and its row SpMM
+ *                          flash-graph/graph_file_header.h:27-37,
+ *                          flash-graph/vertex.h:444-562 (vertex records),
+ *                          flash-graph/utils.cpp:399-420 (file layout),
+ *                          flash-graph/fg_sparse_matrix.cpp:83-106 (run_on_row)
  *   - Hilbert curve        matrix/hilbert_curve.cpp:6-34
  * It is pinned against the reference's own header code compiled in place
  * (oracle/ref_walk.cpp -> oracle/_ref/) and against the golden fixtures in
@@ -754,4 +759,156 @@ double orc_now(void)
 	struct timespec ts;
 	clock_gettime(CLOCK_MONOTONIC, &ts);
 	return ts.tv_sec + ts.tv_nsec * 1e-9;
+}
+
+/* ------------------------------------------------------------------------
+ * The FlashGraph 1D format (test infrastructure: writer and row SpMM)
+ *
+ * File: graph_header, one 4096-byte page (graph_file_header.h:27-37,43:
+ * int64 magic 0x123456789ABCDEF, int version 4, int type (DIRECTED 0,
+ * UNDIRECTED 1, TS_DIRECTED 2, TS_UNDIRECTED 3), size_t num_vertices,
+ * size_t num_edges, int edge_data_size, int max_num_timestamps).  Then one
+ * record per vertex, ids 0..n-1 in order (ext_mem_undirected_vertex,
+ * vertex.h:444-562): u32 id, u32 edge_data_size, u32 num_edges, u32
+ * neighbors[num_edges]; with edge data, the data array starts at
+ * ROUNDUP(12 + 4 num_edges, edge_data_size) and the record ends at
+ * ROUNDUP(that + num_edges * edge_data_size, 4), ROUNDUP(off, base) =
+ * (off + base - 1) & ~(base - 1) (libsafs/common_c.h:36).  A directed graph
+ * stores every vertex's in-edge record, then every out-edge record
+ * (mem_directed_graph::dump_graph, utils.cpp:399-420); an undirected graph
+ * one record per vertex.  Row i of the matrix is vertex i's out-edge record
+ * (the in-edge record for the transpose), fg_sparse_matrix.cpp:473-575.
+ * ------------------------------------------------------------------------ */
+#define ORC_FG_MAGIC 0x123456789ABCDEFLL
+#define ORC_FG_VERSION 4
+
+typedef struct {
+	int64_t magic;
+	int32_t version, type;
+	uint64_t num_vertices, num_edges;
+	int32_t edge_data_size, max_num_timestamps;
+} orc_fg_header;
+
+static uint64_t orc_roundup(uint64_t off, uint64_t base) { return (off + base - 1) & ~(base - 1); }
+
+/* Byte offset of the edge data and total size of a record (vertex.h:458-528). */
+uint64_t orc_fg_data_off(uint32_t ne, uint32_t eds) { return eds ? orc_roundup(12 + 4ull * ne, eds) : 12 + 4ull * ne; }
+uint64_t orc_fg_vsize(uint32_t ne, uint32_t eds)
+{
+	return eds ? orc_roundup(orc_fg_data_off(ne, eds) + (uint64_t)ne * eds, 4) : 12 + 4ull * ne;
+}
+
+typedef struct { uint32_t v, nbr; uint64_t pos; } orc_fg_edge;
+static int cmp_fg_edge(const void *a, const void *b)
+{
+	const orc_fg_edge *x = a, *y = b;
+	if (x->v != y->v) return x->v < y->v ? -1 : 1;
+	if (x->nbr != y->nbr) return x->nbr < y->nbr ? -1 : 1;
+	return x->pos < y->pos ? -1 : (x->pos > y->pos);
+}
+
+static uint64_t orc_fg_put_part(char *out, const orc_fg_edge *e, uint64_t ne, uint64_t nv, const char *vals,
+		uint32_t eds)
+{
+	uint64_t at = 0, i = 0;
+	for (uint64_t v = 0; v < nv; v++) {
+		uint64_t j = i;
+		while (j < ne && e[j].v == v) j++;
+		const uint32_t cnt = (uint32_t)(j - i);
+		char *r = out ? out + at : NULL;
+		if (r) {
+			uint32_t h[3] = {(uint32_t)v, eds, cnt};
+			memcpy(r, h, 12);
+			for (uint64_t q = i; q < j; q++) memcpy(r + 12 + 4 * (q - i), &e[q].nbr, 4);
+			if (eds)
+				for (uint64_t q = i; q < j; q++)
+					memcpy(r + orc_fg_data_off(cnt, eds) + (q - i) * eds, vals + e[q].pos * eds, eds);
+		}
+		at += orc_fg_vsize(cnt, eds);
+		i = j;
+	}
+	return at;
+}
+
+/*
+ * An FlashGraph adjacency image of the edge list: every neighbor list sorted
+ * by id (input order among equal ids), duplicates and self-loops kept, edge
+ * data of `eds` bytes per edge (vals) or none.  *out is malloc'ed (free with
+ * orc_free).  Returns 0 or -1.
+ */
+int orc_fg_build(const uint32_t *src, const uint32_t *dst, const void *vals, uint32_t eds, uint64_t nedges,
+		uint64_t nv, int directed, char **out, uint64_t *out_len)
+{
+	if (eds && !vals) return -1;
+	for (uint64_t i = 0; i < nedges; i++)
+		if (src[i] >= nv || dst[i] >= nv) return -1;
+	/* undirected: the caller lists both directions (as fg's edge lists do) */
+	orc_fg_edge *eo = malloc(sizeof(orc_fg_edge) * (nedges ? nedges : 1));
+	orc_fg_edge *ei = directed ? malloc(sizeof(orc_fg_edge) * (nedges ? nedges : 1)) : NULL;
+	for (uint64_t i = 0; i < nedges; i++) {
+		eo[i].v = src[i]; eo[i].nbr = dst[i]; eo[i].pos = i;
+		if (ei) { ei[i].v = dst[i]; ei[i].nbr = src[i]; ei[i].pos = i; }
+	}
+	qsort(eo, nedges, sizeof(orc_fg_edge), cmp_fg_edge);
+	if (ei) qsort(ei, nedges, sizeof(orc_fg_edge), cmp_fg_edge);
+	uint64_t len = ORC_PAGE + orc_fg_put_part(NULL, eo, nedges, nv, vals, eds);
+	if (ei) len += orc_fg_put_part(NULL, ei, nedges, nv, vals, eds);
+	char *b = calloc(1, len);
+	orc_fg_header h;
+	memset(&h, 0, sizeof(h));
+	h.magic = ORC_FG_MAGIC; h.version = ORC_FG_VERSION; h.type = directed ? 0 : 1;
+	h.num_vertices = nv; h.num_edges = directed ? nedges : nedges / 2; h.edge_data_size = (int32_t)eds;
+	memcpy(b, &h, sizeof(h));
+	uint64_t at = ORC_PAGE;
+	if (ei) at += orc_fg_put_part(b + at, ei, nedges, nv, vals, eds);
+	orc_fg_put_part(b + at, eo, nedges, nv, vals, eds);
+	free(eo); free(ei);
+	*out = b; *out_len = len;
+	return 0;
+}
+
+/*
+ * Y = A X (or A^T X with transpose) over an FlashGraph adjacency image,
+ * fg_row_spmm_task::run_on_row (fg_sparse_matrix.cpp:83-106): per vertex
+ * record, res = 0, then res[j] += X[neighbor][j] * data in record order
+ * (data = 1 without edge data), then Y[id] = res.  `prim` names the edge
+ * data's type (P_BOOL without data).  Returns 0 or -1.
+ */
+int orc_fg_spmm(const char *adj, uint64_t len, int transpose, int prim, int dtype, const void *X, void *Y,
+		uint64_t k)
+{
+	orc_fg_header h;
+	if (len < ORC_PAGE) return -1;
+	memcpy(&h, adj, sizeof(h));
+	if (h.magic != ORC_FG_MAGIC || h.version != ORC_FG_VERSION || (h.type != 0 && h.type != 1)) return -1;
+	const uint64_t nv = h.num_vertices;
+	const uint32_t eds = (uint32_t)h.edge_data_size;
+	const size_t ds = dsize(dtype);
+	uint64_t at = ORC_PAGE;
+	/* a directed graph's in-edge records come first */
+	const int want_in = h.type == 0 && transpose;
+	for (int part = 0; part < (h.type == 0 ? 2 : 1); part++) {
+		const int use = h.type == 0 ? (part == 0) == want_in : 1;
+		for (uint64_t v = 0; v < nv; v++) {
+			uint32_t r[3];
+			if (at + 12 > len) return -1;
+			memcpy(r, adj + at, 12);
+			if (r[0] != v || r[1] != eds) return -1;
+			const uint64_t sz = orc_fg_vsize(r[2], eds);
+			if (at + sz > len) return -1;
+			if (use) {
+				char *y = (char *)Y + v * k * ds;
+				memset(y, 0, k * ds);
+				for (uint32_t i = 0; i < r[2]; i++) {
+					uint32_t c;
+					memcpy(&c, adj + at + 12 + 4ull * i, 4);
+					if (c >= nv) return -1;
+					axpy_row(dtype, y, (const char *)X + (uint64_t)c * k * ds, k,
+							eds ? adj + at + orc_fg_data_off(r[2], eds) + (uint64_t)i * eds : NULL, prim, eds);
+				}
+			}
+			at += sz;
+		}
+	}
+	return 0;
 }

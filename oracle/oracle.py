@@ -8,6 +8,8 @@ and reference legs -- never by the flashx_b200 package.
   libfmx_refwalk.so  oracle/ref_walk.cpp compiled against the reference's own
                      tile headers in place (`make -C oracle ref`, only where the
                      reference tree exists); optional.
+  libfmx_reffg.so    oracle/ref_fg_walk.cpp compiled against FlashGraph's own
+                     vertex record and header classes in place (same rule).
 """
 import ctypes as C
 import os
@@ -18,6 +20,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "liboracle.so")
 REFWALK_SO = os.path.join(HERE, "_ref", "libfmx_refwalk.so")
+REFFG_SO = os.path.join(HERE, "_ref", "libfmx_reffg.so")
 REFERENCE_TREE = "/root/reference"
 
 D_F32, D_F64, D_I32, D_I64 = 0, 1, 3, 4
@@ -65,6 +68,14 @@ def orc():
         L.orc_hilbert_xy2d.restype = i32
         L.orc_hilbert_xy2d.argtypes = [i32, i32, i32]
         L.orc_now.restype = C.c_double
+        L.orc_fg_build.restype = i32
+        L.orc_fg_build.argtypes = [vp, vp, vp, C.c_uint32, u64, u64, i32, C.POINTER(vp), C.POINTER(u64)]
+        L.orc_fg_spmm.restype = i32
+        L.orc_fg_spmm.argtypes = [vp, u64, i32, i32, i32, vp, vp, u64]
+        L.orc_fg_vsize.restype = u64
+        L.orc_fg_vsize.argtypes = [C.c_uint32, C.c_uint32]
+        L.orc_fg_data_off.restype = u64
+        L.orc_fg_data_off.argtypes = [C.c_uint32, C.c_uint32]
         _orc = L
     return _orc
 
@@ -206,3 +217,81 @@ def block_rows_nnz(idx, mat, b0, b1):
 
 def now():
     return orc().orc_now()
+
+
+# ---- the FlashGraph 1D format ------------------------------------------------
+
+def fg_build(src, dst, vals=None, num_vertices=0, directed=True):
+    """FlashGraph adjacency image (bytes) of an edge list: neighbor lists
+    sorted by id, duplicates and self-loops kept; vals (one per edge, any
+    fixed-size dtype) become the edge data.  For an undirected graph list
+    both directions of every edge."""
+    src = np.ascontiguousarray(src, dtype=np.uint32)
+    dst = np.ascontiguousarray(dst, dtype=np.uint32)
+    if not num_vertices:
+        num_vertices = int(max(src.max(initial=0), dst.max(initial=0))) + 1 if len(src) else 0
+    eds, vp = 0, None
+    if vals is not None:
+        vals = np.ascontiguousarray(vals)
+        eds, vp = vals.dtype.itemsize, vals.ctypes.data
+    out, n = C.c_void_p(), C.c_uint64()
+    if orc().orc_fg_build(src.ctypes.data, dst.ctypes.data, vp, eds, len(src), num_vertices, int(directed),
+                          C.byref(out), C.byref(n)):
+        raise ValueError("oracle fg_build failed")
+    b = C.string_at(out, n.value)
+    orc().orc_free(out)
+    return b
+
+
+def fg_spmm(adj, X, transpose=False, edge_prim=P_BOOL):
+    """fg_row_spmm_task over an adjacency image: Y = A X (A^T X)."""
+    X = np.ascontiguousarray(X)
+    X2 = X.reshape(X.shape[0], -1)
+    Y = np.empty_like(X2)
+    if orc().orc_fg_spmm(adj, len(adj), int(transpose), edge_prim, _D_OF[X.dtype], X2.ctypes.data, Y.ctypes.data,
+                         X2.shape[1]):
+        raise ValueError("oracle fg_spmm failed")
+    return Y.reshape(X.shape)
+
+
+def fg_vsize(ne, eds):
+    return orc().orc_fg_vsize(ne, eds)
+
+
+def fg_data_off(ne, eds):
+    return orc().orc_fg_data_off(ne, eds)
+
+
+_reffg = None
+
+
+def reffg():
+    """The walker built from FlashGraph's own headers, or None."""
+    global _reffg
+    if _reffg is None:
+        if not os.path.exists(REFFG_SO):
+            return None
+        L = C.CDLL(REFFG_SO)
+        u64 = C.c_uint64
+        L.ref_fg_header_size.restype = u64
+        L.ref_fg_vsize.restype = u64
+        L.ref_fg_vsize.argtypes = [C.c_uint32, C.c_uint32]
+        L.ref_fg_data_off.restype = u64
+        L.ref_fg_data_off.argtypes = [C.c_uint32, C.c_uint32]
+        L.ref_fg_header.restype = C.c_int
+        L.ref_fg_header.argtypes = [C.c_void_p, C.POINTER(u64), C.POINTER(u64), C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.ref_fg_spmm.restype = C.c_int
+        L.ref_fg_spmm.argtypes = [C.c_void_p, u64, C.c_int, C.c_int, C.c_void_p, C.c_void_p, u64]
+        _reffg = L
+    return _reffg
+
+
+def ref_fg_spmm(adj, X, transpose=False):
+    """The same product through FlashGraph's own record classes (float edge
+    data, FP32 or FP64 operands)."""
+    X = np.ascontiguousarray(X)
+    Y = np.empty_like(X)
+    if reffg().ref_fg_spmm(adj, len(adj), int(transpose), 0 if X.dtype == np.float32 else 1, X.ctypes.data,
+                           Y.ctypes.data, X.shape[1]):
+        raise ValueError("reference FlashGraph walker failed")
+    return Y
