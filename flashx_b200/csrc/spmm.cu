@@ -133,6 +133,19 @@ struct gpu_part {
 	void *partial = nullptr;
 	uint64_t hot_entries = 0;            // entries that read the hot pack
 	uint64_t bytes = 0;
+	// streamed part: the entry stream stays in pinned host memory and each
+	// SpMM copies it slice by slice into two device slots (copy_st), the
+	// kernel of one slice overlapping the copy of the next
+	struct slice_t { uint64_t e0, e1; uint32_t r0, nr; };   // entries [e0, e1), ranges [r0, r0 + nr)
+	bool streamed = false;
+	uint32_t *h_col = nullptr;
+	void *h_val = nullptr;
+	std::vector<slice_t> slices;
+	uint32_t *slot_col[2] = {nullptr, nullptr};
+	void *slot_val[2] = {nullptr, nullptr};
+	cudaStream_t copy_st = nullptr;
+	cudaEvent_t ev_start = nullptr, ev_copied[2] = {nullptr, nullptr}, ev_free[2] = {nullptr, nullptr};
+	uint64_t host_bytes = 0;
 	// staging buffers of fmx_spmm_host (grow-only, guarded by stage_mu)
 	std::mutex stage_mu;
 	void *stage_x = nullptr, *stage_y = nullptr;
@@ -141,9 +154,15 @@ struct gpu_part {
 		int cur = 0;
 		cudaGetDevice(&cur);
 		cudaSetDevice(device);
-		void *ps[] = {col, val, hot_col, xhot, ranges, heavy, partial, stage_x, stage_y};
+		void *ps[] = {col, val, hot_col, xhot, ranges, heavy, partial, stage_x, stage_y, slot_col[0], slot_col[1],
+				slot_val[0], slot_val[1]};
 		for (void *p : ps)
 			if (p) cudaFree(p);
+		if (h_col) cudaFreeHost(h_col);
+		if (h_val) cudaFreeHost(h_val);
+		for (cudaEvent_t e : {ev_start, ev_copied[0], ev_copied[1], ev_free[0], ev_free[1]})
+			if (e) cudaEventDestroy(e);
+		if (copy_st) cudaStreamDestroy(copy_st);
 		cudaSetDevice(cur);
 	}
 };
@@ -862,7 +881,43 @@ static void par_for(uint64_t n, F fn)
 	for (auto &x : th) x.join();
 }
 
-static int make_part(const host_csr &csr, int device, std::shared_ptr<gpu_part> &out)
+// A streamed part's pinned host copy of the entry stream, its two device
+// slots (the largest slice plus kStep entries, zeroed) and its copy stream
+// and events.  Called with the part's device current.
+static int stream_buffers(gpu_part &p, const std::vector<uint32_t> &col, const std::vector<char> &val, size_t es)
+{
+	uint64_t cap = 0;
+	for (const auto &sl : p.slices) cap = std::max<uint64_t>(cap, sl.e1 - sl.e0);
+	cap += kStep;
+	auto host = [&](void **h, const void *src, size_t n) -> int {
+		cudaError_t e = cudaHostAlloc(h, std::max<size_t>(n, 16), cudaHostAllocDefault);
+		if (e != cudaSuccess) return set_error(FMX_ERR_OOM, "pinned host stream of %zu bytes: %s", n, cudaGetErrorString(e));
+		if (n) memcpy(*h, src, n);
+		p.host_bytes += n;
+		return FMX_OK;
+	};
+	if (int rc = host(reinterpret_cast<void **>(&p.h_col), col.data(), col.size() * sizeof(uint32_t))) return rc;
+	if (es)
+		if (int rc = host(&p.h_val, val.data(), val.size())) return rc;
+	for (int b = 0; b < 2; b++) {
+		CUDA_TRY(cudaMalloc(&p.slot_col[b], cap * sizeof(uint32_t)));
+		CUDA_TRY(cudaMemset(p.slot_col[b], 0, cap * sizeof(uint32_t)));
+		p.bytes += cap * sizeof(uint32_t);
+		if (es) {
+			CUDA_TRY(cudaMalloc(&p.slot_val[b], cap * es));
+			CUDA_TRY(cudaMemset(p.slot_val[b], 0, cap * es));
+			p.bytes += cap * es;
+		}
+		CUDA_TRY(cudaEventCreateWithFlags(&p.ev_copied[b], cudaEventDisableTiming));
+		CUDA_TRY(cudaEventCreateWithFlags(&p.ev_free[b], cudaEventDisableTiming));
+	}
+	CUDA_TRY(cudaEventCreateWithFlags(&p.ev_start, cudaEventDisableTiming));
+	CUDA_TRY(cudaStreamCreateWithFlags(&p.copy_st, cudaStreamNonBlocking));
+	return FMX_OK;
+}
+
+// slice_entries > 0: a streamed part whose slices hold about that many entries.
+static int make_part(const host_csr &csr, int device, std::shared_ptr<gpu_part> &out, uint64_t slice_entries = 0)
 {
 	if (csr.ncols > (1ull << 30))
 		return set_error(FMX_ERR_UNSUPPORTED, "%llu columns: the entry stream holds 30-bit column ids",
@@ -951,9 +1006,25 @@ static int make_part(const host_csr &csr, int device, std::shared_ptr<gpu_part> 
 	for (size_t i = 0; i < segs.size(); i++)
 		ranges[i] = {uint32_t(segs[i].at), segs[i].len, uint32_t(segs[i].row0), segs[i].slot};
 	// largest ranges first, so that round-robin assignment balances the groups
-	std::stable_sort(ranges.begin(), ranges.end(), [](const range_t &x, const range_t &y) {
-		return x.len > y.len;
-	});
+	// (within each slice of a streamed part: a slice is whole segments in
+	// stream order, at least slice_entries entries but the last)
+	auto by_len = [](const range_t &x, const range_t &y) { return x.len > y.len; };
+	if (slice_entries) {
+		p->streamed = true;
+		uint64_t e0 = 0;
+		size_t i0 = 0;
+		for (size_t i = 0; i < segs.size(); i++) {
+			const uint64_t e1 = segs[i].at + segs[i].len;
+			if (e1 - e0 >= slice_entries || i + 1 == segs.size()) {
+				p->slices.push_back({e0, e1, uint32_t(i0), uint32_t(i + 1 - i0)});
+				std::stable_sort(ranges.begin() + i0, ranges.begin() + i + 1, by_len);
+				e0 = e1;
+				i0 = i + 1;
+			}
+		}
+	} else {
+		std::stable_sort(ranges.begin(), ranges.end(), by_len);
+	}
 
 	// the entry stream (plus kStep entries so that index prefetches stay in bounds)
 	const size_t padded = total + kStep;
@@ -998,11 +1069,15 @@ static int make_part(const host_csr &csr, int device, std::shared_ptr<gpu_part> 
 	CUDA_TRY(cudaSetDevice(device));
 	int rc = FMX_OK;
 	uint64_t &bytes = p->bytes;
-	rc = upload(&p->col, col.data(), col.size(), bytes, padded);
-	if (!rc && es) {
-		char *v = nullptr;
-		rc = upload(&v, val.data(), val.size(), bytes, padded * es);
-		p->val = v;
+	if (p->streamed) {
+		rc = stream_buffers(*p, col, val, es);
+	} else {
+		rc = upload(&p->col, col.data(), col.size(), bytes, padded);
+		if (!rc && es) {
+			char *v = nullptr;
+			rc = upload(&v, val.data(), val.size(), bytes, padded * es);
+			p->val = v;
+		}
 	}
 	if (!rc) rc = upload(&p->hot_col, hot_col.data(), hot_col.size(), bytes);
 	if (!rc) rc = upload(&p->ranges, ranges.data(), ranges.size(), bytes);
@@ -1051,6 +1126,44 @@ static unsigned persistent_blocks(K kernel, int device)
 #define FMX_SPMM_STEP 4                  // entries gathered per stream step (4 or 8)
 #endif
 
+// Run launch(args) over the part's ranges: once for a resident entry stream;
+// slice by slice for a streamed part.  Each slice is copied from pinned host
+// memory into one of two device slots on the part's copy stream; the kernel
+// of slice i (on st) waits for its copy, and the copy of slice i + 2 waits
+// for that kernel, so copies overlap the kernels.  The slot pointer is
+// rebased by the slice's first entry, so the ranges keep their absolute
+// entry offsets.  The slots are the part's scratch: calls on one part must
+// not overlap on the GPU (as for the hot pack and the partial sums).
+template <class F>
+static int over_slices(const gpu_part &p, spmm_args a, cudaStream_t st, F &&launch)
+{
+	if (!p.streamed) return launch(a);
+	gpu_part &q = const_cast<gpu_part &>(p);
+	CUDA_TRY(cudaEventRecord(q.ev_start, st));
+	CUDA_TRY(cudaStreamWaitEvent(q.copy_st, q.ev_start, 0));
+	for (size_t i = 0; i < p.slices.size(); i++) {
+		const gpu_part::slice_t &sl = p.slices[i];
+		const int b = int(i & 1);
+		if (i >= 2) CUDA_TRY(cudaStreamWaitEvent(q.copy_st, q.ev_free[b], 0));
+		const uint64_t ne = sl.e1 - sl.e0;
+		CUDA_TRY(cudaMemcpyAsync(q.slot_col[b], p.h_col + sl.e0, ne * sizeof(uint32_t), cudaMemcpyHostToDevice,
+				q.copy_st));
+		if (p.esize)
+			CUDA_TRY(cudaMemcpyAsync(q.slot_val[b], static_cast<const char *>(p.h_val) + sl.e0 * p.esize,
+					ne * p.esize, cudaMemcpyHostToDevice, q.copy_st));
+		CUDA_TRY(cudaEventRecord(q.ev_copied[b], q.copy_st));
+		CUDA_TRY(cudaStreamWaitEvent(st, q.ev_copied[b], 0));
+		a.col = q.slot_col[b] - sl.e0;
+		a.val = p.esize ? static_cast<const void *>(static_cast<const char *>(q.slot_val[b]) - sl.e0 * p.esize)
+				: nullptr;
+		a.ranges = p.ranges + sl.r0;
+		a.n_ranges = sl.nr;
+		if (int rc = launch(a)) return rc;
+		CUDA_TRY(cudaEventRecord(q.ev_free[b], st));
+	}
+	return FMX_OK;
+}
+
 template <class XT, class YT, class A, class WT, int VEC, int NV, bool SI, bool SO>
 static int launch_one(const gpu_part &p, const spmm_args &a, cudaStream_t st)
 {
@@ -1075,11 +1188,12 @@ static int launch_t(const gpu_part &p, spmm_args a, bool sin, bool sout, cudaStr
 				a.ldx, a.k, static_cast<XT *>(p.xhot), a.hot_ld, nullptr);
 		CUDA_TRY(cudaGetLastError());
 	}
-	int rc;
-	if (sin && sout) rc = launch_one<XT, YT, A, WT, VEC, NV, true, true>(p, a, st);
-	else if (sin) rc = launch_one<XT, YT, A, WT, VEC, NV, true, false>(p, a, st);
-	else if (sout) rc = launch_one<XT, YT, A, WT, VEC, NV, false, true>(p, a, st);
-	else rc = launch_one<XT, YT, A, WT, VEC, NV, false, false>(p, a, st);
+	int rc = over_slices(p, a, st, [&](const spmm_args &sa) -> int {
+		if (sin && sout) return launch_one<XT, YT, A, WT, VEC, NV, true, true>(p, sa, st);
+		if (sin) return launch_one<XT, YT, A, WT, VEC, NV, true, false>(p, sa, st);
+		if (sout) return launch_one<XT, YT, A, WT, VEC, NV, false, true>(p, sa, st);
+		return launch_one<XT, YT, A, WT, VEC, NV, false, false>(p, sa, st);
+	});
 	if (rc) return rc;
 	if (sout) rc = launch_fixup<YT, A, true>(p, static_cast<const A *>(a.partial), static_cast<YT *>(a.Y), a.ldy, a.k,
 			static_cast<const A *>(a.s_out), st);
@@ -1113,8 +1227,12 @@ static int run_spmv(const gpu_part &p, const T *X, int64_t ldx, T *Y, int64_t ld
 	static unsigned blocks[64] = {0};
 	unsigned &b = blocks[p.device & 63];
 	if (!b) b = persistent_blocks(kern, p.device);
-	kern<<<b, kThreads, 0, st>>>(a, e);
-	CUDA_TRY(cudaGetLastError());
+	if (int rc = over_slices(p, a, st, [&](const spmm_args &sa) -> int {
+			kern<<<b, kThreads, 0, st>>>(sa, e);
+			CUDA_TRY(cudaGetLastError());
+			return FMX_OK;
+		}))
+		return rc;
 	return launch_fixup<T, T, false, EPI>(p, static_cast<const T *>(p.partial), Y, ldy, 1, nullptr, st, e);
 }
 
@@ -1402,6 +1520,48 @@ int fmx_matrix_create(const fmx_image *img, const fmx_image *t_img, int device, 
 	}
 	m->symmetric = (t_img == nullptr);
 	*out = m.release();
+	return FMX_OK;
+}
+
+int fmx_matrix_create_streamed(const fmx_image *img, const fmx_image *t_img, int device, uint64_t slice_entries,
+		fmx_matrix **out)
+{
+	if (!img || !out) return set_error(FMX_ERR_INVAL, "null argument");
+	*out = nullptr;
+	if (!slice_entries) slice_entries = uint64_t(1) << 26;
+	int ndev = 0;
+	if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+		return set_error(FMX_ERR_CUDA, "no CUDA device is available");
+	if (device < 0 || device >= ndev) return set_error(FMX_ERR_INVAL, "device %d out of range (%d devices)", device, ndev);
+	if (t_img && (t_img->im.h.nrows != img->im.h.ncols || t_img->im.h.ncols != img->im.h.nrows))
+		return set_error(FMX_ERR_DIM, "transpose image is %llux%llu, expected %llux%llu",
+				(unsigned long long)t_img->im.h.nrows, (unsigned long long)t_img->im.h.ncols,
+				(unsigned long long)img->im.h.ncols, (unsigned long long)img->im.h.nrows);
+	std::unique_ptr<fmx_matrix> m(new (std::nothrow) fmx_matrix);
+	if (!m) return set_error(FMX_ERR_OOM, "out of host memory");
+	const fmx_image *parts[2] = {img, t_img};
+	for (int i = 0; i < 2; i++) {
+		if (!parts[i]) continue;
+		host_csr csr;
+		int rc;
+		try {
+			rc = decode_to_csr(parts[i]->im, csr, default_threads());
+			if (!rc) rc = make_part(csr, device, i == 0 ? m->a : m->at, slice_entries);
+		} catch (const std::bad_alloc &) {
+			rc = set_error(FMX_ERR_OOM, "host allocation failed while decoding the image");
+		}
+		if (rc) return rc;
+	}
+	m->symmetric = (t_img == nullptr);
+	*out = m.release();
+	return FMX_OK;
+}
+
+int fmx_matrix_stream_info(const fmx_matrix *m, uint64_t *slices, uint64_t *host_bytes)
+{
+	if (!m || !m->a) return set_error(FMX_ERR_INVAL, "null matrix");
+	if (slices) *slices = m->a->streamed ? m->a->slices.size() : 0;
+	if (host_bytes) *host_bytes = m->a->host_bytes;
 	return FMX_OK;
 }
 
@@ -1699,6 +1859,7 @@ extern "C" int fmx_spmm_noalloc(const fmx_matrix *m, const float *X, int64_t ldx
 	if (k <= 0 || ldx < k || ldy < k) return set_error(FMX_ERR_DIM, "bad k (%lld) or leading dimensions", (long long)k);
 	if (p.prim != FMX_P_BOOL && p.prim != FMX_P_FLOAT)
 		return set_error(FMX_ERR_TYPE, "fmx_spmm_noalloc takes binary or float-weighted matrices");
+	if (p.streamed) return set_error(FMX_ERR_UNSUPPORTED, "fmx_spmm_noalloc takes matrices resident in HBM");
 	// scratch layout: the hot pack (widest panel), then the long-row partial sums
 	const size_t hot_bytes = (size_t(p.n_hot + 1) * kPanelBytes + 255) / 256 * 256;
 	const size_t need = hot_bytes + size_t(p.n_partials) * kPartialStride * sizeof(float);

@@ -200,6 +200,23 @@ class sparse_matrix:
         return cls(h.value, device)
 
     @classmethod
+    def create_streamed(cls, index, t_index=None, device=0, slice_entries=0):
+        """The semi-external form (sparse_matrix::create(index, mat_io_factory),
+        sparse_matrix.cpp:693-707): from matrix_image(s), the entry stream kept
+        in pinned host memory and streamed to the GPU in slices of about
+        slice_entries entries (0: 2^26) during every multiply."""
+        h = C.c_void_p()
+        check(lib.fmx_matrix_create_streamed(index._h, t_index._h if t_index is not None else None, device,
+                                             int(slice_entries), C.byref(h)))
+        return cls(h.value, device)
+
+    def stream_info(self):
+        """(slices per SpMM, pinned host bytes); (0, 0) for a resident matrix."""
+        a, b = C.c_uint64(), C.c_uint64()
+        check(lib.fmx_matrix_stream_info(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    @classmethod
     def load(cls, mat_idx_file, mat_file, t_mat_idx_file=None, t_mat_file=None, device=0):
         h = C.c_void_p()
         enc = lambda s: s.encode() if s is not None else None

@@ -115,6 +115,20 @@ int fmx_image_free(fmx_image *img);
  */
 int fmx_matrix_create(const fmx_image *img, const fmx_image *t_img, int device,
                       fmx_matrix **out);
+/* The semi-external form: sparse_matrix::create(SpM_2d_index::ptr,
+ * safs::file_io_factory::shared_ptr[, t_index, t_mat_io_fac])
+ * (matrix/sparse_matrix.cpp:693-707) keeps the tiles in SAFS and reads them
+ * during every multiply.  Here the matrix's entry stream (column ids and
+ * values) stays in pinned host memory and every SpMM streams it to the GPU in
+ * slices of about slice_entries entries (0: 2^26), copying one slice while
+ * the kernel runs on the previous one; the schedule, the hot-column pack and
+ * the partial sums stay in HBM.  For matrices whose entry stream does not fit
+ * in HBM beside the dense operands.  Results are identical to
+ * fmx_matrix_create's. */
+int fmx_matrix_create_streamed(const fmx_image *img, const fmx_image *t_img, int device,
+                               uint64_t slice_entries, fmx_matrix **out);
+/* Slices per SpMM (0 for a resident matrix) and pinned host bytes held. */
+int fmx_matrix_stream_info(const fmx_matrix *m, uint64_t *slices, uint64_t *host_bytes);
 /* Build the resident matrix straight from an edge list in the memory of
  * `device` (src_dev, dst_dev: uint32 ids; vals_dev: nedges values of
  * val_type, or NULL for FMX_P_BOOL): the sort, deduplication and row
