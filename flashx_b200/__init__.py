@@ -9,5 +9,14 @@ from .sparse_matrix import (  # noqa: F401
     SpM_2d_index, SpM_2d_storage, create_2d_matrix, matrix_image, set_deduplicate,
     set_remove_self_edge, sparse_matrix)
 
+
+
+def release_cached(device=0):
+    """Hand the solvers' reserved device workspace back to the driver
+    (fmx_release_cached; as torch.cuda.empty_cache does for torch's cache)."""
+    from ._lib import check
+    check(lib.fmx_release_cached(int(device)))
+
+
 __all__ = ["FmxError", "SpM_2d_index", "SpM_2d_storage", "create_2d_matrix", "matrix_image",
-           "set_deduplicate", "set_remove_self_edge", "sparse_matrix"]
+           "release_cached", "set_deduplicate", "set_remove_self_edge", "sparse_matrix"]

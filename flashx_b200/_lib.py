@@ -103,6 +103,7 @@ _SIGS = {
     "fmx_matrix_build_device": (_int, [_vp, _vp, _vp, _int, _u64, _u64, _u64, _int, _int, _vp, _P(_vp)]),
     "fmx_matrix_from_fg": (_int, [_vp, _sz, _int, _int, _P(_vp)]),
     "fmx_matrix_create_streamed": (_int, [_vp, _vp, _int, _u64, _P(_vp)]),
+    "fmx_release_cached": (_int, [_int]),
     "fmx_matrix_stream_info": (_int, [_vp, _P(_u64), _P(_u64)]),
     "fmx_matrix_load_fg": (_int, [C.c_char_p, _int, _int, _P(_vp)]),
     "fmx_eigen_default_options": (None, [_P(eigen_options_t), _int]),

@@ -118,7 +118,7 @@ struct dbuf {
 	int get(T **out, size_t count)
 	{
 		void *q = nullptr;
-		cudaError_t e = cudaMallocAsync(&q, std::max<size_t>(count, 1) * sizeof(T), st);
+		cudaError_t e = work_alloc(&q, std::max<size_t>(count, 1) * sizeof(T), st);
 		if (e != cudaSuccess) return set_error(FMX_ERR_OOM, "device builder: %zu bytes: %s", count * sizeof(T),
 				cudaGetErrorString(e));
 		p.push_back(q);

@@ -393,7 +393,7 @@ struct workspace {
 	int get(T **p, size_t count)
 	{
 		void *q = nullptr;
-		cudaError_t e = cudaMallocAsync(&q, std::max<size_t>(count, 1) * sizeof(T), st);
+		cudaError_t e = work_alloc(&q, std::max<size_t>(count, 1) * sizeof(T), st);
 		if (e != cudaSuccess)
 			return set_error(FMX_ERR_OOM, "eigensolver workspace of %zu bytes: %s", count * sizeof(T),
 					cudaGetErrorString(e));

@@ -94,6 +94,10 @@ int edges_to_csr_device(const uint32_t *src, const uint32_t *dst, const void *va
 
 int default_threads();
 
+// Stream-ordered workspace from the current device's library pool (freed
+// memory stays reserved for the next call; fmx_release_cached returns it).
+cudaError_t work_alloc(void **p, size_t bytes, cudaStream_t st);
+
 // A matrix from host CSR (and its transpose, or null for a symmetric one).
 int matrix_from_csr(const host_csr &a, const host_csr *at, int device, fmx_matrix **out);
 

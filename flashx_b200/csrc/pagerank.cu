@@ -108,7 +108,7 @@ int fmx_pagerank(const fmx_matrix *m, uint64_t max_iters, float damping, float *
 	uint32_t *mask;
 	unsigned long long *state;
 	auto alloc = [&](void **q, size_t bytes) -> int {
-		cudaError_t e = cudaMallocAsync(q, std::max<size_t>(bytes, 16), st);
+		cudaError_t e = work_alloc(q, std::max<size_t>(bytes, 16), st);
 		if (e != cudaSuccess) return set_error(FMX_ERR_OOM, "PageRank vectors: %s", cudaGetErrorString(e));
 		g.bufs.push_back(*q);
 		return FMX_OK;

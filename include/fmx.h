@@ -176,6 +176,12 @@ int fmx_matrix_device_bytes(const fmx_matrix *m, uint64_t *bytes);
 int fmx_matrix_transpose(const fmx_matrix *m, fmx_matrix **out);
 int fmx_matrix_free(fmx_matrix *m);
 
+/* The solvers (fmx_eigen_solve, fmx_pagerank, the GNN, the device builder)
+ * take their device workspace from one memory pool per device that keeps
+ * freed memory reserved for the next call.  Hand it back to the driver (as
+ * torch.cuda.empty_cache does for torch's cache). */
+int fmx_release_cached(int device);
+
 /* ---- SpMM -----------------------------------------------------------------
  * Y = diag(row_scale_out) * A * diag(row_scale_in) * X   (scales nullable)
  * Replaces sparse_matrix::multiply(in, out) (matrix/sparse_matrix.cpp:709-771)

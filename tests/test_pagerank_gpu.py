@@ -108,3 +108,18 @@ def test_pagerank_fused_matches_stepwise_loop(torch_cuda):
         got, git = PageRank(m, cap, 0.85)
         assert git == min(cap, it)
         assert np.array_equal(got.cpu().numpy(), ref[git - 1])
+
+
+def test_workspace_pool_release(torch_cuda):
+    """The solvers' workspace pool keeps freed memory for the next call;
+    release_cached hands it back, and later calls still run."""
+    torch = torch_cuda
+    from flashx_b200 import release_cached
+    n = 6000
+    src, dst = _directed(n, 50000, 11)
+    m = create_2d_matrix(src, dst, None, block_size=(1024, 1024), is_sym=False, nrows=n, ncols=n)
+    p1, i1 = PageRank(m, 30, 0.85)
+    release_cached(0)
+    p2, i2 = PageRank(m, 30, 0.85)
+    assert i1 == i2 and torch.equal(p1, p2)
+    release_cached(0)
