@@ -129,6 +129,7 @@ struct gpu_part {
 	heavy_row *heavy = nullptr;
 	uint32_t n_heavy = 0;
 	uint32_t n_long_heavy = 0;           // the first heavy rows, of more than kLongChunks chunks
+	uint32_t n_block_heavy = 0;          // the first of those, of more than kBlockChunks chunks
 	uint32_t n_partials = 0;
 	void *partial = nullptr;
 	uint64_t hot_entries = 0;            // entries that read the hot pack
@@ -735,6 +736,107 @@ __global__ void pack_hot_kernel(const int32_t *hot_col, uint32_t n_hot, const XT
 	}
 }
 
+// Part `part` of P adds chunks part, part + P, ... of one column unit (a
+// float4 when vec, else one element) into two running sums (even and odd
+// steps).
+template <class A>
+__device__ __forceinline__ void chunk_sums(const A *pc, uint32_t part, uint32_t P, uint32_t count, bool vec,
+		A (&s0)[4], A (&s1)[4])
+{
+	constexpr bool kVec4 = std::is_same<A, float>::value;
+	uint32_t c = part;
+	for (; c + P < count; c += 2u * P) {
+		if constexpr (kVec4) {
+			if (vec) {
+				const float4 a = *reinterpret_cast<const float4 *>(pc + int64_t(c) * kPartialStride);
+				const float4 b = *reinterpret_cast<const float4 *>(pc + int64_t(c + P) * kPartialStride);
+				s0[0] = acc_add(s0[0], a.x); s0[1] = acc_add(s0[1], a.y);
+				s0[2] = acc_add(s0[2], a.z); s0[3] = acc_add(s0[3], a.w);
+				s1[0] = acc_add(s1[0], b.x); s1[1] = acc_add(s1[1], b.y);
+				s1[2] = acc_add(s1[2], b.z); s1[3] = acc_add(s1[3], b.w);
+				continue;
+			}
+		}
+		s0[0] = acc_add(s0[0], pc[int64_t(c) * kPartialStride]);
+		s1[0] = acc_add(s1[0], pc[int64_t(c + P) * kPartialStride]);
+	}
+	if (c < count) {
+		if constexpr (kVec4) {
+			if (vec) {
+				const float4 a = *reinterpret_cast<const float4 *>(pc + int64_t(c) * kPartialStride);
+				s0[0] = acc_add(s0[0], a.x); s0[1] = acc_add(s0[1], a.y);
+				s0[2] = acc_add(s0[2], a.z); s0[3] = acc_add(s0[3], a.w);
+				return;
+			}
+		}
+		s0[0] = acc_add(s0[0], pc[int64_t(c) * kPartialStride]);
+	}
+}
+
+// The longest heavy rows (more than kBlockChunks chunks, the first n_block of
+// the list): a block of 8 warps per row, 8 * 32 / L parts, each warp's parts
+// combined by the xor tree and the 8 warp sums added in warp order.  The
+// chain of one part is then at most count / (8 * 32 / L) chunks long instead
+// of count / (32 / L), which bounded the whole fixup by its longest row.
+constexpr uint32_t kBlockChunks = 64;
+template <class YT, class A, bool SCALE_OUT, bool EPI = false>
+__global__ void __launch_bounds__(256) spmm_fixup_block_kernel(const heavy_row *heavy, const A *partial, YT *Y,
+		int64_t ldy, int k, const A *s_out, int L, const pr_epi e)
+{
+	if constexpr (EPI) {
+		if (e.state[1]) return;
+	}
+	__shared__ A red[8][32][4];
+	constexpr bool kVec4 = std::is_same<A, float>::value;
+	const bool vec = kVec4 && (k % 4) == 0;
+	const int units = vec ? k / 4 : k;
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	const int per_warp = 32 / L;
+	const int P = 8 * per_warp;
+	const int cl = lane % L, part = warp * per_warp + lane / L;
+	const heavy_row h = heavy[blockIdx.x];
+	for (int u0 = 0; u0 < units; u0 += L) {           // the same trip count on every thread
+		const int u = u0 + cl;
+		const bool mine = u < units;
+		A s0[4] = {A(0), A(0), A(0), A(0)}, s1[4] = {A(0), A(0), A(0), A(0)};
+		if (mine) chunk_sums<A>(partial + int64_t(h.first) * kPartialStride + (vec ? 4 * u : u), uint32_t(part),
+				uint32_t(P), h.count, vec, s0, s1);
+		A t[4];
+#pragma unroll
+		for (int i = 0; i < 4; i++) t[i] = acc_add(s0[i], s1[i]);
+		for (int o = L; o < 32; o <<= 1)
+#pragma unroll
+			for (int i = 0; i < 4; i++) t[i] = acc_add(t[i], __shfl_xor_sync(0xffffffffu, t[i], o));
+		if (lane < L)
+#pragma unroll
+			for (int i = 0; i < 4; i++) red[warp][lane][i] = t[i];
+		__syncthreads();
+		if (warp == 0 && lane < L && mine) {
+			A v[4];
+#pragma unroll
+			for (int i = 0; i < 4; i++) {
+				v[i] = red[0][lane][i];
+				for (int w = 1; w < 8; w++) v[i] = acc_add(v[i], red[w][lane][i]);
+			}
+			if constexpr (EPI) {
+				unsigned c = 0;
+				pr_update(e, h.row, v[0], c);
+				if (c) atomicAdd(e.state, 1ull);
+			} else {
+				A so = A(1);
+				if constexpr (SCALE_OUT) so = s_out[h.row];
+				YT *y = Y + int64_t(h.row) * ldy + (vec ? 4 * u : u);
+				for (int i = 0; i < (vec ? 4 : 1); i++) {
+					A x = v[i];
+					if constexpr (SCALE_OUT) x = acc_mul(x, so);
+					y[i] = from_acc<YT, A>(x);
+				}
+			}
+		}
+		__syncthreads();
+	}
+}
+
 // Heavy rows: add the chunk partials, scale, convert, store.  A row's
 // columns are covered by L lanes (L = k / 4 float4 lanes for FP32 panels of
 // k % 4 == 0, else one lane per column, rounded up to a power of two, at most
@@ -768,38 +870,8 @@ __global__ void spmm_fixup_kernel(const heavy_row *heavy, uint32_t n_heavy, uint
 		const int u = u0 + cl;
 		const bool mine = live && u < units;
 		A s0[4] = {A(0), A(0), A(0), A(0)}, s1[4] = {A(0), A(0), A(0), A(0)};
-		if (mine) {
-			const A *pc = partial + int64_t(h.first) * kPartialStride + (vec ? 4 * u : u);
-			uint32_t c = uint32_t(part);
-			for (; c + uint32_t(P) < h.count; c += 2u * uint32_t(P)) {
-				if constexpr (kVec4) {
-					if (vec) {
-						const float4 a = *reinterpret_cast<const float4 *>(pc + int64_t(c) * kPartialStride);
-						const float4 b = *reinterpret_cast<const float4 *>(pc + int64_t(c + P) * kPartialStride);
-						s0[0] = acc_add(s0[0], a.x); s0[1] = acc_add(s0[1], a.y);
-						s0[2] = acc_add(s0[2], a.z); s0[3] = acc_add(s0[3], a.w);
-						s1[0] = acc_add(s1[0], b.x); s1[1] = acc_add(s1[1], b.y);
-						s1[2] = acc_add(s1[2], b.z); s1[3] = acc_add(s1[3], b.w);
-						continue;
-					}
-				}
-				s0[0] = acc_add(s0[0], pc[int64_t(c) * kPartialStride]);
-				s1[0] = acc_add(s1[0], pc[int64_t(c + P) * kPartialStride]);
-			}
-			if (c < h.count) {
-				if constexpr (kVec4) {
-					if (vec) {
-						const float4 a = *reinterpret_cast<const float4 *>(pc + int64_t(c) * kPartialStride);
-						s0[0] = acc_add(s0[0], a.x); s0[1] = acc_add(s0[1], a.y);
-						s0[2] = acc_add(s0[2], a.z); s0[3] = acc_add(s0[3], a.w);
-					} else {
-						s0[0] = acc_add(s0[0], pc[int64_t(c) * kPartialStride]);
-					}
-				} else {
-					s0[0] = acc_add(s0[0], pc[int64_t(c) * kPartialStride]);
-				}
-			}
-		}
+		if (mine) chunk_sums<A>(partial + int64_t(h.first) * kPartialStride + (vec ? 4 * u : u), uint32_t(part),
+				uint32_t(P), h.count, vec, s0, s1);
 		const int nv = vec ? 4 : 1;
 		A t[4];
 #pragma unroll
@@ -837,12 +909,19 @@ static int launch_fixup(const gpu_part &p, const A *partial, YT *Y, int64_t ldy,
 	const int units = vec ? k / 4 : k;
 	int L = 1;
 	while (L < units && L < 32) L <<= 1;
+	const uint32_t nb = p.n_block_heavy;
+	if (nb) {
+		spmm_fixup_block_kernel<YT, A, SCALE_OUT, EPI><<<nb, 256, 0, st>>>(p.heavy, partial, Y, ldy, k, s_out, L, e);
+		CUDA_TRY(cudaGetLastError());
+	}
+	if (p.n_heavy == nb) return FMX_OK;
+	const uint64_t n_long = p.n_long_heavy - nb;
 	const uint64_t n_short = p.n_heavy - p.n_long_heavy;
 	const uint64_t per_warp = uint64_t(32 / (L * (L < 32 ? 2 : 1)));    // short rows per warp
-	const uint64_t warps = p.n_long_heavy + (n_short + per_warp - 1) / per_warp;
+	const uint64_t warps = n_long + (n_short + per_warp - 1) / per_warp;
 	const unsigned fb = unsigned((warps * 32 + 255) / 256);
-	spmm_fixup_kernel<YT, A, SCALE_OUT, EPI><<<fb, 256, 0, st>>>(p.heavy, p.n_heavy, p.n_long_heavy, partial, Y,
-			ldy, k, s_out, L, e);
+	spmm_fixup_kernel<YT, A, SCALE_OUT, EPI><<<fb, 256, 0, st>>>(p.heavy + nb, p.n_heavy - nb, uint32_t(n_long),
+			partial, Y, ldy, k, s_out, L, e);
 	CUDA_TRY(cudaGetLastError());
 	return FMX_OK;
 }
@@ -1086,6 +1165,8 @@ static int make_part(const host_csr &csr, int device, std::shared_ptr<gpu_part> 
 	std::stable_sort(heavy.begin(), heavy.end(), [](const heavy_row &x, const heavy_row &y) { return x.count > y.count; });
 	p->n_long_heavy = uint32_t(std::count_if(heavy.begin(), heavy.end(),
 			[](const heavy_row &h) { return h.count > kLongChunks; }));
+	p->n_block_heavy = uint32_t(std::count_if(heavy.begin(), heavy.end(),
+			[](const heavy_row &h) { return h.count > kBlockChunks; }));
 	if (!rc) rc = upload(&p->heavy, heavy.data(), heavy.size(), bytes);
 	p->n_hot = uint32_t(hot_col.size());
 	p->n_exact = n_exact;
