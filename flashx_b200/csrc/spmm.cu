@@ -1775,10 +1775,17 @@ int fmx_spmm_host(const fmx_matrix *m, int x_type, const void *X_host, int64_t l
 	if (!rc) rc = grow(p.stage_y, p.stage_yb, yb);
 	cudaStream_t st = nullptr;
 	if (!rc && cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) rc = set_error(FMX_ERR_CUDA, "stream creation failed");
-	if (!rc && cudaMemcpy2DAsync(p.stage_x, k * xs, X_host, ldx * xs, k * xs, p.ncols, cudaMemcpyHostToDevice, st) != cudaSuccess)
+	// one linear copy each way when the rows are contiguous (a pitched copy
+	// of 64-byte rows moves far below the link rate)
+	auto copy = [&](void *dst, size_t dpitch, const void *src, size_t spitch, size_t width, size_t rows,
+			cudaMemcpyKind kind) {
+		if (dpitch == width && spitch == width) return cudaMemcpyAsync(dst, src, width * rows, kind, st);
+		return cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, rows, kind, st);
+	};
+	if (!rc && copy(p.stage_x, k * xs, X_host, ldx * xs, k * xs, p.ncols, cudaMemcpyHostToDevice) != cudaSuccess)
 		rc = set_error(FMX_ERR_CUDA, "copy of X to the device failed");
 	if (!rc) rc = spmm_part(p, x_type, p.stage_x, k, y_type, p.stage_y, k, k, nullptr, nullptr, st);
-	if (!rc && cudaMemcpy2DAsync(Y_host, ldy * ys, p.stage_y, k * ys, k * ys, p.nrows, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+	if (!rc && copy(Y_host, ldy * ys, p.stage_y, k * ys, k * ys, p.nrows, cudaMemcpyDeviceToHost) != cudaSuccess)
 		rc = set_error(FMX_ERR_CUDA, "copy of Y to the host failed");
 	if (st) {
 		cudaError_t e = cudaStreamSynchronize(st);
@@ -1807,7 +1814,8 @@ int fmx_matrix_schedule(const fmx_matrix *m, uint64_t *n_light_rows, uint64_t *n
 	if (n_light_rows) *n_light_rows = p.n_exact;
 	if (n_split_tasks) *n_split_tasks = p.n_ranges;
 	if (n_heavy_rows) *n_heavy_rows = p.n_heavy;
-	if (kernels_per_spmm) *kernels_per_spmm = 2 + (p.n_heavy ? 1 : 0);
+	if (kernels_per_spmm)
+		*kernels_per_spmm = 2 + (p.n_block_heavy ? 1 : 0) + (p.n_heavy > p.n_block_heavy ? 1 : 0);
 	return FMX_OK;
 }
 
