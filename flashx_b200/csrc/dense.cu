@@ -554,6 +554,81 @@ gram_f64_kernel(const float *__restrict__ X, int64_t ldx, int M, const float *__
 	}
 }
 
+// FP64 Gram for M, N <= 16 on the FP64 tensor path (mma.sync m8n8k4 .f64):
+// a warp takes 4 rows per step (the MMA's K).  Lane (g = lane / 4,
+// t = lane % 4) holds x[r][g] and x[r][8 + g] for r = row + t (A fragments
+// of the two 8-row halves of x^T) and the same of w (B fragments), so every
+// input element is loaded and converted once; 4 MMAs update the 2 x 2 tiles
+// of G.  Products of FP32 inputs are exact in FP64.  The 8 warps' tiles are
+// added in warp order (deterministic for a fixed grid).
+__device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b)
+{
+	asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+			: "+d"(d[0]), "+d"(d[1]) : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(256)
+gram_dmma_kernel(const float *__restrict__ X, int64_t ldx, int M, const float *__restrict__ W, int64_t ldw, int N,
+		int64_t n, double *__restrict__ part)
+{
+	__shared__ double red[8][16 * 16];
+	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+	const int g = lane >> 2, t = lane & 3;
+	double c[2][2][2];
+#pragma unroll
+	for (int mi = 0; mi < 2; mi++)
+#pragma unroll
+		for (int ni = 0; ni < 2; ni++) c[mi][ni][0] = c[mi][ni][1] = 0.0;
+	const int64_t steps = (n + 3) / 4;
+	const int64_t nw = int64_t(gridDim.x) * 8;
+	int64_t q = int64_t(blockIdx.x) * 8 + warp;
+	// two steps per trip: all loads first
+	for (; q + nw < steps; q += 2 * nw) {
+		double a[2][2], bb[2][2];
+#pragma unroll
+		for (int u = 0; u < 2; u++) {
+			const int64_t r = 4 * (q + u * nw) + t;
+			const bool rv = r < n;
+			a[u][0] = (rv && g < M) ? double(X[r * ldx + g]) : 0.0;
+			a[u][1] = (rv && 8 + g < M) ? double(X[r * ldx + 8 + g]) : 0.0;
+			bb[u][0] = (rv && g < N) ? double(W[r * ldw + g]) : 0.0;
+			bb[u][1] = (rv && 8 + g < N) ? double(W[r * ldw + 8 + g]) : 0.0;
+		}
+#pragma unroll
+		for (int u = 0; u < 2; u++)
+#pragma unroll
+			for (int mi = 0; mi < 2; mi++)
+#pragma unroll
+				for (int ni = 0; ni < 2; ni++) dmma_8x8x4(c[mi][ni], a[u][mi], bb[u][ni]);
+	}
+	for (; q < steps; q += nw) {
+		const int64_t r = 4 * q + t;
+		const bool rv = r < n;
+		const double a0 = (rv && g < M) ? double(X[r * ldx + g]) : 0.0;
+		const double a1 = (rv && 8 + g < M) ? double(X[r * ldx + 8 + g]) : 0.0;
+		const double b0 = (rv && g < N) ? double(W[r * ldw + g]) : 0.0;
+		const double b1 = (rv && 8 + g < N) ? double(W[r * ldw + 8 + g]) : 0.0;
+		dmma_8x8x4(c[0][0], a0, b0);
+		dmma_8x8x4(c[0][1], a0, b1);
+		dmma_8x8x4(c[1][0], a1, b0);
+		dmma_8x8x4(c[1][1], a1, b1);
+	}
+	// D fragment: G[8 mi + g][8 ni + 2 t + i]
+#pragma unroll
+	for (int mi = 0; mi < 2; mi++)
+#pragma unroll
+		for (int ni = 0; ni < 2; ni++)
+#pragma unroll
+			for (int i = 0; i < 2; i++) red[warp][(8 * mi + g) * 16 + 8 * ni + 2 * t + i] = c[mi][ni][i];
+	__syncthreads();
+	for (int pr = tid; pr < M * N; pr += 256) {
+		const int i = pr / N, j = pr % N;
+		double sum = red[0][i * 16 + j];
+		for (int w = 1; w < 8; w++) sum += red[w][i * 16 + j];
+		part[size_t(blockIdx.x) * M * N + pr] = sum;
+	}
+}
+
 // ---------------------------------------------------------------------------
 // Small FP64 problems on one CTA (b <= 64)
 // ---------------------------------------------------------------------------
@@ -750,7 +825,10 @@ int fmx_dense_gram(int precision, const float *X, int64_t ldx, int M, const floa
 	cudaStream_t st = static_cast<cudaStream_t>(stream);
 	const int parts = fmx_dense_gram_parts(precision, n);
 	if (precision == FMX_DENSE_F64) {
-		gram_f64_kernel<<<parts, 256, 0, st>>>(X, ldx, M, W, ldw, N, n, static_cast<double *>(part));
+		if (M <= 16 && N <= 16)
+			gram_dmma_kernel<<<parts, 256, 0, st>>>(X, ldx, M, W, ldw, N, n, static_cast<double *>(part));
+		else
+			gram_f64_kernel<<<parts, 256, 0, st>>>(X, ldx, M, W, ldw, N, n, static_cast<double *>(part));
 		DCUDA_TRY(cudaGetLastError());
 		gram_reduce_kernel<double><<<(M * N + 7) / 8, 256, 0, st>>>(static_cast<const double *>(part), parts, M * N,
 				static_cast<double *>(G));

@@ -231,3 +231,25 @@ def test_svd_operator_rectangular(torch_cuda, precision):
     sv, vt = sv[order], vt[order]
     np.testing.assert_allclose(res.vals, sv[:4] ** 2, rtol=1e-6)
     assert _sin_angle(X, vt[:4].T) <= 1e-4
+
+
+@pytest.mark.parametrize("block", [10, 12, 24])
+def test_block_sizes_off_sixteen(torch_cuda, block):
+    """Blocks of 10 and 12 columns take the FP64 tensor-path basis update and
+    Gram with guarded (non-vector) loads; 24 takes the CUDA-core kernels."""
+    n, B = 8000, 4
+    src, dst, _ = sbm_edges(n, B, 20.0, 20.0, seed=5)
+    N, _, _ = _na(n, src, dst)
+    m = _matrix(n, src, dst)
+    opts = eigen_options()
+    opts.init(B)
+    opts.block_size = block
+    opts.which = "LA"
+    opts.tol = TOL
+    res = compute_eigen(NA_operator(m), True, opts)
+    assert res.status.converged == B and res.status.max_residual <= TOL
+    vals = np.asarray(res.vals, dtype=np.float64)
+    X = res.vecs.double().cpu().numpy()
+    assert float(_residuals(N, vals, X).max()) <= 2 * TOL
+    w = eigsh(N, k=B, which="LA", tol=1e-10, return_eigenvectors=False)
+    assert np.allclose(np.sort(vals), np.sort(w), atol=1e-6)
