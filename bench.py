@@ -319,7 +319,7 @@ def streamed_measure(img, X, Y, dev, reps=5):
     """The semi-external form at the bench workload: the entry stream in
     pinned host memory, streamed to the GPU in slices of 2^26 entries during
     every SpMM.  Its bound is the host-to-device copy rate, measured here
-    with one 1 GiB pinned copy."""
+    as the best of three 1 GiB pinned copies."""
     import torch
     from flashx_b200 import sparse_matrix
     t = time.time()
@@ -343,18 +343,21 @@ def streamed_measure(img, X, Y, dev, reps=5):
     d = torch.empty(1 << 28, dtype=torch.float32, device=dev)
     d.copy_(h, non_blocking=True)
     torch.cuda.synchronize(dev)
-    c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    c0.record(stream)
-    d.copy_(h, non_blocking=True)
-    c1.record(stream)
-    torch.cuda.synchronize(dev)
-    h2d = (1 << 30) / (c0.elapsed_time(c1) / 1e3) / 1e9
+    rates = []
+    for _ in range(3):
+        c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        c0.record(stream)
+        d.copy_(h, non_blocking=True)
+        c1.record(stream)
+        torch.cuda.synchronize(dev)
+        rates.append((1 << 30) / (c0.elapsed_time(c1) / 1e3) / 1e9)
+    h2d = max(rates)
     achieved = host_bytes / (ms / 1e3) / 1e9
     del m, h, d
     return {"slice_entries": 1 << 26, "slices": int(slices), "stream_bytes_per_spmm": int(host_bytes),
             "ms_per_spmm": round(ms, 3), "create_s": round(create_s, 2), "identical_to_resident": identical,
             "roofline": {"bound": "pcie_h2d", "achieved": round(achieved, 2), "peak": round(h2d, 2), "unit": "GB/s",
-                         "frac": round(achieved / h2d, 4), "peak_kind": "measured here: one 1 GiB pinned copy"}}
+                         "frac": round(achieved / h2d, 4), "peak_kind": "measured here: best of three 1 GiB pinned copies"}}
 
 
 def pagerank_measure(a, dev):
