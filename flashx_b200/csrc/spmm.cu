@@ -1203,6 +1203,20 @@ static unsigned persistent_blocks(K kernel, int device)
 	return unsigned(std::max(1, sms) * std::max(1, per));
 }
 
+// The persistent grid of `kernel` on `device`, kept in `slot` (one array of
+// slots per kernel instantiation, indexed by device; racing first calls
+// compute the same value).
+template <class K>
+static unsigned cached_blocks(std::atomic<unsigned> &slot, K kernel, int device)
+{
+	unsigned b = slot.load(std::memory_order_relaxed);
+	if (!b) {
+		b = persistent_blocks(kernel, device);
+		slot.store(b, std::memory_order_relaxed);
+	}
+	return b;
+}
+
 #ifndef FMX_SPMM_STEP
 #define FMX_SPMM_STEP 4                  // entries gathered per stream step (4 or 8)
 #endif
@@ -1249,9 +1263,8 @@ template <class XT, class YT, class A, class WT, int VEC, int NV, bool SI, bool 
 static int launch_one(const gpu_part &p, const spmm_args &a, cudaStream_t st)
 {
 	auto kern = spmm_kernel<XT, YT, A, WT, VEC, NV, FMX_SPMM_STEP, SI, SO>;
-	static unsigned blocks[64] = {0};
-	unsigned &b = blocks[p.device & 63];
-	if (!b) b = persistent_blocks(kern, p.device);
+	static std::atomic<unsigned> blocks[64];
+	const unsigned b = cached_blocks(blocks[p.device & 63], kern, p.device);
 	kern<<<b, kThreads, 0, st>>>(a, pr_epi{});
 	CUDA_TRY(cudaGetLastError());
 	return FMX_OK;
@@ -1305,9 +1318,8 @@ static int run_spmv(const gpu_part &p, const T *X, int64_t ldx, T *Y, int64_t ld
 			nullptr);
 	CUDA_TRY(cudaGetLastError());
 	auto kern = spmv_kernel<T, WT, EPI>;
-	static unsigned blocks[64] = {0};
-	unsigned &b = blocks[p.device & 63];
-	if (!b) b = persistent_blocks(kern, p.device);
+	static std::atomic<unsigned> blocks[64];
+	const unsigned b = cached_blocks(blocks[p.device & 63], kern, p.device);
 	if (int rc = over_slices(p, a, st, [&](const spmm_args &sa) -> int {
 			kern<<<b, kThreads, 0, st>>>(sa, e);
 			CUDA_TRY(cudaGetLastError());
