@@ -134,12 +134,16 @@ def cpu_sample(img, a, nthreads, target_s, reps=None):
     nb = oracle.num_block_rows(idx)
     rng = np.random.default_rng(3)
     X = rng.standard_normal((inf["ncols"], a.k)).astype(np.float32)
-    # calibrate on one block row, then grow the sample to the target time
-    b1 = 1
+    # calibrate on two block rows per thread, then size the sample to the
+    # target time: a multiple of the thread count, at least four block rows
+    # per thread (block rows are the unit the workers take), so that every
+    # thread stays busy
+    bc = int(min(nb, 2 * nthreads))
     t = time.perf_counter()
-    oracle.spmm(idx, mat, X, nthreads=nthreads, brows=(0, b1))
-    dt = max(time.perf_counter() - t, 1e-4)
-    b1 = int(min(nb, max(1, target_s / dt)))
+    oracle.spmm(idx, mat, X, nthreads=nthreads, brows=(0, bc))
+    dt = max(time.perf_counter() - t, 1e-4) / bc
+    b1 = int(target_s / dt) // nthreads * nthreads
+    b1 = int(min(nb, max(4 * nthreads, b1)))
     nnz_s = oracle.block_rows_nnz(idx, mat, 0, b1)
     times = []
     for _ in range(reps or 1):
@@ -471,7 +475,8 @@ def run_reference(a, rank, world):
     nthreads, model = cpu_info()
     inf = img.info()
     # each step is a bounded sample of the workload: the whole run (warm-up
-    # included) holds about 90 s of CPU work, at least one block row per step
+    # included) holds about 90 s of CPU work, at least four block rows per
+    # host thread per step
     warm = a.warmup
     per = min(0.5, 90.0 / max(a.steps + warm, 1))
     gbs, sample, times = cpu_sample(img, a, nthreads, per, reps=a.steps + warm)
