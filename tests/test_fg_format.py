@@ -90,3 +90,63 @@ def test_fg_matches_2d_like_the_reference_unit_test(directed, with_attr):
     X = (np.arange(n * 10, dtype=np.float64).reshape(n, 10)).astype(np.float32)   # in_mat[i][j] = 10 i + j
     prim = oracle.P_FLOAT if with_attr else oracle.P_BOOL
     assert np.array_equal(oracle.fg_spmm(adj, X, False, prim), oracle.spmm(idx, mat, X))
+
+
+def _from_fg(adj, prim):
+    import ctypes as C
+    from flashx_b200 import _lib
+    h = C.c_void_p()
+    rc = _lib.lib.fmx_matrix_from_fg(adj, len(adj), prim, 0, C.byref(h))
+    return rc, h
+
+
+def test_product_loader_validates_on_the_host():
+    """fmx_matrix_from_fg parses and checks the image before it needs a GPU:
+    malformed images are rejected here with the reference's error classes,
+    and a valid one gets as far as the device (FMX_ERR_CUDA without one)."""
+    import torch
+    from flashx_b200 import _lib
+    n = 300
+    s, d, w = _edges(3, n, 2000, False, True)
+    adj = oracle.fg_build(s, d, w, n, directed=True)
+    bad = bytearray(adj)
+    bad[0] ^= 1                                          # magic
+    assert _from_fg(bytes(bad), _lib.P_FLOAT)[0] == _lib.FMX_ERR_IMAGE
+    ver = bytearray(adj)
+    ver[8:12] = (3).to_bytes(4, "little")                # version
+    assert _from_fg(bytes(ver), _lib.P_FLOAT)[0] == _lib.FMX_ERR_IMAGE
+    ts = bytearray(adj)
+    ts[12:16] = (3).to_bytes(4, "little")                # TS_UNDIRECTED
+    assert _from_fg(bytes(ts), _lib.P_FLOAT)[0] == _lib.FMX_ERR_UNSUPPORTED
+    assert _from_fg(adj, _lib.P_BOOL)[0] == _lib.FMX_ERR_TYPE      # 4-byte edge data
+    assert _from_fg(adj, _lib.P_DOUBLE)[0] == _lib.FMX_ERR_TYPE
+    assert _from_fg(adj[:-4], _lib.P_FLOAT)[0] == _lib.FMX_ERR_IMAGE   # truncated
+    assert _from_fg(adj[:100], _lib.P_FLOAT)[0] == _lib.FMX_ERR_IMAGE  # no header page
+    nb = bytearray(adj)
+    first = 4096 + 12                                    # first neighbor of vertex 0's in-record
+    nb[first:first + 4] = (n + 5).to_bytes(4, "little")
+    if int.from_bytes(adj[4096 + 8:4096 + 12], "little"):          # vertex 0 has in-edges
+        assert _from_fg(bytes(nb), _lib.P_FLOAT)[0] == _lib.FMX_ERR_IMAGE
+    ids = bytearray(adj)
+    ids[4096:4100] = (7).to_bytes(4, "little")           # record 0 names vertex 7
+    assert _from_fg(bytes(ids), _lib.P_FLOAT)[0] == _lib.FMX_ERR_IMAGE
+    if not torch.cuda.is_available():
+        assert _from_fg(adj, _lib.P_FLOAT)[0] == _lib.FMX_ERR_CUDA
+
+
+def test_device_entry_points_check_arguments_on_the_host():
+    """The device builder and the streamed form reject bad arguments before
+    they touch a GPU."""
+    import ctypes as C
+    from flashx_b200 import _lib
+    h = C.c_void_p()
+    L = _lib.lib
+    # flags outside DEDUP | KEEP_SELF_LOOPS | TRANSPOSE
+    assert L.fmx_matrix_build_device(None, None, None, _lib.P_BOOL, 0, 4, 4, 0x4, 0, None, C.byref(h)) \
+        == _lib.FMX_ERR_INVAL
+    # edges without arrays, values of a weighted type without a value array
+    assert L.fmx_matrix_build_device(None, None, None, _lib.P_BOOL, 10, 4, 4, 0, 0, None, C.byref(h)) \
+        == _lib.FMX_ERR_INVAL
+    assert L.fmx_matrix_create_streamed(None, None, 0, 0, C.byref(h)) == _lib.FMX_ERR_INVAL
+    assert L.fmx_matrix_stream_info(None, None, None) == _lib.FMX_ERR_INVAL
+    assert L.fmx_release_cached(-1) == _lib.FMX_ERR_INVAL
