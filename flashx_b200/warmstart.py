@@ -5,7 +5,8 @@ SpMM and the tcgen05 dense kernels, BF16 operands, FP32 accumulation) maps
 vertex features (standardised log-degree plus 15 N(0,1) channels, propagated
 three times by D^-1/2 A D^-1/2) to a 16-column start block.  It is trained on
 eigenvectors that the plain solver computes on generated SBM graphs; the
-randomly started plain solver stays the fallback and the judge of residual.
+randomly started plain solver stays the fallback, and every residual is
+recomputed by the solver itself.
 
     net = warm_start_net(seed=0)
     net.train(instances, epochs=4)            # instances: sbm_instance(...)

@@ -34,7 +34,7 @@ enum fmx_status {
 	FMX_ERR_OOM = -5,        /* host or device allocation failed              */
 	FMX_ERR_CUDA = -6,       /* a CUDA runtime call failed                    */
 	FMX_ERR_IO = -7,         /* file could not be opened / read / written     */
-	FMX_ERR_UNSUPPORTED = -8 /* valid request this build does not implement   */
+	FMX_ERR_UNSUPPORTED = -8 /* valid request the library does not implement  */
 };
 
 /* ---- element types ----------------------------------------------------- */

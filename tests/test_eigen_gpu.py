@@ -1,7 +1,7 @@
 """The block eigensolver (fmx_eigen_solve) against FP64 references.
 
 There is no eigensolver in the reference tree to pin against (its iterations
-live in the external Trilinos Anasazi), so each result is judged by:
+live in the external Trilinos Anasazi), so each result is checked by:
   * the residual ||A x - l x|| / ||A|| of every returned pair, recomputed here
     in FP64 with scipy (not with the library's SpMM): <= tol (1e-6) x 2;
   * eigenvalues against scipy's ARPACK (FP64): |l - l_ref| <= 1e-6;
