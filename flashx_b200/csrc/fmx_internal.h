@@ -98,6 +98,24 @@ int default_threads();
 // memory stays reserved for the next call; fmx_release_cached returns it).
 cudaError_t work_alloc(void **p, size_t bytes, cudaStream_t st);
 
+// The device a matrix lives on.
+int matrix_device(const fmx_matrix *m);
+// Makes `device` current for its lifetime and then restores the caller's.
+struct device_guard {
+	int prev = -1;
+	explicit device_guard(int device)
+	{
+		int cur = 0;
+		if (cudaGetDevice(&cur) == cudaSuccess && cur != device && cudaSetDevice(device) == cudaSuccess) prev = cur;
+	}
+	~device_guard()
+	{
+		if (prev >= 0) cudaSetDevice(prev);
+	}
+	device_guard(const device_guard &) = delete;
+	device_guard &operator=(const device_guard &) = delete;
+};
+
 // A matrix from host CSR (and its transpose, or null for a symmetric one).
 int matrix_from_csr(const host_csr &a, const host_csr *at, int device, fmx_matrix **out);
 

@@ -1560,6 +1560,8 @@ __global__ void rmat_kernel(rmat_params p, uint64_t n, uint32_t *src, uint32_t *
 	}
 }
 
+int matrix_device(const fmx_matrix *m) { return m && m->a ? m->a->device : 0; }
+
 int matrix_from_csr(const host_csr &a, const host_csr *at, int device, fmx_matrix **out)
 {
 	*out = nullptr;
