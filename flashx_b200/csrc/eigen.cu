@@ -312,35 +312,38 @@ __device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b)
 			: "+d"(d[0]), "+d"(d[1]) : "d"(a), "d"(b));
 }
 
-// The basis update of ritz_kernel for b <= 16 on the FP64 tensor path: a warp
-// takes 8 rows per step (the MMA's M).  The 16 input columns are the MMA's K
-// in 4 steps, relabelled so that lane t's A element at step s is column
-// 4 t + s (one 16-byte load per row and operand); V' = V[:, perm] (zero
-// beyond b) sits in 8 B-fragment registers per lane for the whole kernel.
-// Two 8-column tiles give X (and NX from W); lane (g, t) ends with columns
-// 2t, 2t + 1, 8 + 2t, 9 + 2t of row 8 * tile + g.  Products of FP32 inputs
+// The basis update of ritz_kernel for b <= 8 NT (NT = 2 or 4 column tiles of
+// 8) on the FP64 tensor path: a warp takes 8 rows per step (the MMA's M).
+// The input columns are the MMA's K in 2 NT steps, relabelled so that lane
+// t's A element at step s is column 16 (s / 4) + 4 t + s % 4 (one 16-byte
+// load per row, operand and 16 columns); V' = V[:, perm] (zero beyond b)
+// sits in 2 NT x NT B-fragment registers per lane for the whole kernel.
+// NT 8-column tiles give X (and NX from W); lane (g, t) ends with columns
+// 8 ni + 2t, 8 ni + 2t + 1 of row 8 * tile + g.  Products of FP32 inputs
 // are exact in FP64; residual sums are reduced over lanes, then warps, in a
 // fixed order.  Same outputs and partial layout as ritz_kernel.
-template <bool HAS_W, bool RES, bool WRITE>
+template <int NT, bool HAS_W, bool RES, bool WRITE>
 __global__ void __launch_bounds__(kThreads)
 ritz_dmma_kernel(const float *__restrict__ Q, const float *__restrict__ W, int b, const double *__restrict__ V,
 		const int *__restrict__ perm, const double *__restrict__ theta, float *__restrict__ X,
 		float *__restrict__ NX, int64_t n, double *__restrict__ part, int resid_out, bool vec)
 {
-	__shared__ double red[kThreads / 32][32];
+	constexpr int KS = 2 * NT;                // k-steps of 4 columns
+	constexpr int H = NT / 2;                 // 16-column halves
+	__shared__ double red[kThreads / 32][64];
 	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 	const int g = lane >> 2, t = lane & 3;
-	double vb[4][2];
+	double vb[KS][NT];
 #pragma unroll
-	for (int st = 0; st < 4; st++)
+	for (int st = 0; st < KS; st++)
 #pragma unroll
-		for (int ni = 0; ni < 2; ni++) {
-			const int k = 4 * t + st, j = 8 * ni + g;
+		for (int ni = 0; ni < NT; ni++) {
+			const int k = 16 * (st / 4) + 4 * t + st % 4, j = 8 * ni + g;
 			vb[st][ni] = (k < b && j < b) ? V[k * b + (perm ? perm[j] : j)] : 0.0;
 		}
-	double th[2][2], racc[2][2], xacc[2][2];
+	double th[NT][2], racc[NT][2], xacc[NT][2];
 #pragma unroll
-	for (int ni = 0; ni < 2; ni++)
+	for (int ni = 0; ni < NT; ni++)
 #pragma unroll
 		for (int i = 0; i < 2; i++) {
 			const int j = 8 * ni + 2 * t + i;
@@ -352,37 +355,45 @@ ritz_dmma_kernel(const float *__restrict__ Q, const float *__restrict__ W, int b
 			tile += int64_t(gridDim.x) * (kThreads / 32)) {
 		const int64_t row = tile * 8 + g;
 		const bool rv = row < n;
-		float qa[4] = {0.f, 0.f, 0.f, 0.f}, wa[4] = {0.f, 0.f, 0.f, 0.f};
-		if (rv) {
-			if (vec) {
-				const float4 qv = *reinterpret_cast<const float4 *>(Q + row * 16 + 4 * t);
-				qa[0] = qv.x; qa[1] = qv.y; qa[2] = qv.z; qa[3] = qv.w;
-				if (HAS_W) {
-					const float4 wv = *reinterpret_cast<const float4 *>(W + row * 16 + 4 * t);
-					wa[0] = wv.x; wa[1] = wv.y; wa[2] = wv.z; wa[3] = wv.w;
-				}
-			} else {
+		float qa[KS], wa[KS];
 #pragma unroll
-				for (int st = 0; st < 4; st++)
-					if (4 * t + st < b) {
-						qa[st] = Q[row * b + 4 * t + st];
-						if (HAS_W) wa[st] = W[row * b + 4 * t + st];
+		for (int st = 0; st < KS; st++) qa[st] = wa[st] = 0.f;
+		if (rv) {
+#pragma unroll
+			for (int h = 0; h < H; h++) {
+				const int c0 = 16 * h + 4 * t;
+				if (vec && c0 + 3 < b) {
+					const float4 qv = *reinterpret_cast<const float4 *>(Q + row * b + c0);
+					qa[4 * h] = qv.x; qa[4 * h + 1] = qv.y; qa[4 * h + 2] = qv.z; qa[4 * h + 3] = qv.w;
+					if (HAS_W) {
+						const float4 wv = *reinterpret_cast<const float4 *>(W + row * b + c0);
+						wa[4 * h] = wv.x; wa[4 * h + 1] = wv.y; wa[4 * h + 2] = wv.z; wa[4 * h + 3] = wv.w;
 					}
+				} else {
+#pragma unroll
+					for (int e = 0; e < 4; e++)
+						if (c0 + e < b) {
+							qa[4 * h + e] = Q[row * b + c0 + e];
+							if (HAS_W) wa[4 * h + e] = W[row * b + c0 + e];
+						}
+				}
 			}
 		}
-		double cx[2][2] = {{0.0, 0.0}, {0.0, 0.0}}, cy[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+		double cx[NT][2], cy[NT][2];
 #pragma unroll
-		for (int st = 0; st < 4; st++) {
+		for (int ni = 0; ni < NT; ni++) cx[ni][0] = cx[ni][1] = cy[ni][0] = cy[ni][1] = 0.0;
+#pragma unroll
+		for (int st = 0; st < KS; st++) {
 			const double aq = qa[st], aw = wa[st];
 #pragma unroll
-			for (int ni = 0; ni < 2; ni++) {
+			for (int ni = 0; ni < NT; ni++) {
 				dmma_8x8x4(cx[ni], aq, vb[st][ni]);
 				if (HAS_W) dmma_8x8x4(cy[ni], aw, vb[st][ni]);
 			}
 		}
 		if (WRITE && rv) {
 #pragma unroll
-			for (int ni = 0; ni < 2; ni++) {
+			for (int ni = 0; ni < NT; ni++) {
 				const int j = 8 * ni + 2 * t;
 				float2 xo, yo;
 				xo.x = float(cx[ni][0]); xo.y = float(cx[ni][1]);
@@ -390,9 +401,9 @@ ritz_dmma_kernel(const float *__restrict__ Q, const float *__restrict__ W, int b
 					yo.x = float(resid_out ? cy[ni][0] - th[ni][0] * cx[ni][0] : cy[ni][0]);
 					yo.y = float(resid_out ? cy[ni][1] - th[ni][1] * cx[ni][1] : cy[ni][1]);
 				}
-				if (vec) {
-					*reinterpret_cast<float2 *>(X + row * 16 + j) = xo;
-					if (HAS_W) *reinterpret_cast<float2 *>(NX + row * 16 + j) = yo;
+				if (vec && j + 1 < b) {
+					*reinterpret_cast<float2 *>(X + row * b + j) = xo;
+					if (HAS_W) *reinterpret_cast<float2 *>(NX + row * b + j) = yo;
 				} else {
 					if (j < b) {
 						X[row * b + j] = xo.x;
@@ -408,7 +419,7 @@ ritz_dmma_kernel(const float *__restrict__ Q, const float *__restrict__ W, int b
 		if (RES) {
 			// rows beyond n had zero inputs: they add nothing
 #pragma unroll
-			for (int ni = 0; ni < 2; ni++)
+			for (int ni = 0; ni < NT; ni++)
 #pragma unroll
 				for (int i = 0; i < 2; i++) {
 					const double d = cy[ni][i] - th[ni][i] * cx[ni][i];
@@ -420,7 +431,7 @@ ritz_dmma_kernel(const float *__restrict__ Q, const float *__restrict__ W, int b
 	if (RES) {
 		// lanes of one t hold the same columns: add over g (lane bits 2-4)
 #pragma unroll
-		for (int ni = 0; ni < 2; ni++)
+		for (int ni = 0; ni < NT; ni++)
 #pragma unroll
 			for (int i = 0; i < 2; i++)
 				for (int o = 4; o < 32; o <<= 1) {
@@ -429,15 +440,15 @@ ritz_dmma_kernel(const float *__restrict__ Q, const float *__restrict__ W, int b
 				}
 		if (lane < 4)
 #pragma unroll
-			for (int ni = 0; ni < 2; ni++)
+			for (int ni = 0; ni < NT; ni++)
 #pragma unroll
 				for (int i = 0; i < 2; i++) {
 					red[warp][8 * ni + 2 * t + i] = racc[ni][i];
-					red[warp][16 + 8 * ni + 2 * t + i] = xacc[ni][i];
+					red[warp][32 + 8 * ni + 2 * t + i] = xacc[ni][i];
 				}
 		__syncthreads();
 		for (int i = tid; i < 2 * b; i += kThreads) {
-			const int slot = i < b ? i : 16 + (i - b);
+			const int slot = i < b ? i : 32 + (i - b);
 			double sum = 0;
 			for (int w2 = 0; w2 < kThreads / 32; w2++) sum += red[w2][slot];
 			part[size_t(blockIdx.x) * 2 * b + i] = sum;
@@ -445,16 +456,20 @@ ritz_dmma_kernel(const float *__restrict__ Q, const float *__restrict__ W, int b
 	}
 }
 
-// ritz_kernel or, for b <= 16, ritz_dmma_kernel
+// ritz_kernel or, for b <= 32, ritz_dmma_kernel
 template <bool HAS_W, bool RES, bool WRITE>
 static void launch_ritz(int grid, cudaStream_t st, const float *Q, const float *W, int b, const double *V,
 		const int *perm, const double *theta, float *X, float *NX, int64_t n, double *part, int resid_out)
 {
 	auto al = [](const void *p, uintptr_t a) { return (reinterpret_cast<uintptr_t>(p) & (a - 1)) == 0; };
-	// 16-byte row loads and 8-byte column-pair stores when b = 16 and aligned
-	const bool vec = b == 16 && al(Q, 16) && al(W, 16) && al(X, 8) && al(NX, 8);
+	// 16-byte row loads and 8-byte column-pair stores when every row starts
+	// on a 16-byte boundary (b % 4 == 0) and the bases are aligned
+	const bool vec = b % 4 == 0 && al(Q, 16) && al(W, 16) && al(X, 8) && al(NX, 8);
 	if (b <= 16)
-		ritz_dmma_kernel<HAS_W, RES, WRITE><<<grid, kThreads, 0, st>>>(Q, W, b, V, perm, theta, X, NX, n, part,
+		ritz_dmma_kernel<2, HAS_W, RES, WRITE><<<grid, kThreads, 0, st>>>(Q, W, b, V, perm, theta, X, NX, n, part,
+				resid_out, vec);
+	else if (b <= 32)
+		ritz_dmma_kernel<4, HAS_W, RES, WRITE><<<grid, kThreads, 0, st>>>(Q, W, b, V, perm, theta, X, NX, n, part,
 				resid_out, vec);
 	else
 		ritz_kernel<HAS_W, RES, WRITE><<<grid, kThreads, 0, st>>>(Q, W, b, V, perm, theta, X, NX, n, part, resid_out);
@@ -632,10 +647,10 @@ struct solver {
 		E_TRY(ws.get(&tc_err, 1));
 		E_TRY(ws.get(&info, 4));
 		E_TRY(ws.get(&dsmall, 1));
-		// rows per CTA and pass: 8 per warp on the FP64 tensor path (b <= 16),
+		// rows per CTA and pass: 8 per warp on the FP64 tensor path (b <= 32),
 		// else one row per 1, 2 or 4 threads
-		const int R = b <= 16 ? 8 * (kThreads / 32) : kThreads / ritz_threads_per_row(b);
-		ritz_grid = int(std::max<int64_t>(1, std::min<int64_t>((n + R - 1) / R, int64_t(sm_count()) * (b <= 16 ? 4 : 2))));
+		const int R = b <= 32 ? 8 * (kThreads / 32) : kThreads / ritz_threads_per_row(b);
+		ritz_grid = int(std::max<int64_t>(1, std::min<int64_t>((n + R - 1) / R, int64_t(sm_count()) * (b <= 32 ? 4 : 2))));
 		E_TRY(ws.get(&part, size_t(ritz_grid) * 2 * b));
 		const int gparts = std::max({fmx_dense_gram_parts(FMX_DENSE_F64, n), fmx_dense_gram_parts(FMX_DENSE_TF32X3, n)});
 		E_TRY(ws.get(&gpart, size_t(gparts) * b * b * 2));      // room for double partials

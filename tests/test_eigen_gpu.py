@@ -233,10 +233,11 @@ def test_svd_operator_rectangular(torch_cuda, precision):
     assert _sin_angle(X, vt[:4].T) <= 1e-4
 
 
-@pytest.mark.parametrize("block", [10, 12, 24])
+@pytest.mark.parametrize("block", [10, 12, 20, 24, 32])
 def test_block_sizes_off_sixteen(torch_cuda, block):
-    """Blocks of 10 and 12 columns take the FP64 tensor-path basis update and
-    Gram with guarded (non-vector) loads; 24 takes the CUDA-core kernels."""
+    """Blocks of up to 32 columns take the FP64 tensor-path basis update (one
+    or two 16-column halves, guarded loads past b); the Gram takes the FP64
+    MMA kernel up to 16 columns and the CUDA-core kernel beyond."""
     n, B = 8000, 4
     src, dst, _ = sbm_edges(n, B, 20.0, 20.0, seed=5)
     N, _, _ = _na(n, src, dst)
