@@ -25,7 +25,8 @@ to the oracle's CPU restatement, and at scale 22 on the GPU.
 
 --impl reference times the reference's CPU SpMM algorithm (the oracle's C
 restatement of FlashMatrix's 2D traversal; the reference library itself
-cannot be built here) on all host cores over a bounded sample of block rows.
+cannot be built here) on all host cores, one whole-matrix SpMM per step, in a
+process that loads only the oracle (its own R-MAT stream and image builder).
 Under torchrun every rank runs an independent replica (the path does not
 need a data exchange); value = all ranks' bytes / max rank time.
 """
@@ -123,40 +124,106 @@ def cpu_info():
     return os.cpu_count() or 1, model
 
 
-def cpu_sample(img, a, nthreads, target_s, reps=None):
-    """Time the oracle (the reference's CPU SpMM algorithm) on the first block
-    rows of the image holding ~target_s seconds of work; returns GB/s scaled to
-    the full matrix's B_alg per nnz, plus a description of the sample."""
+def oracle_mod():
+    """The CPU oracle (test infrastructure): the reference's CPU SpMM, builder
+    and PageRank restated in C; loaded only by the CPU legs of this bench."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
-    idx, mat = img.bytes()
-    inf = img.info()
-    nb = oracle.num_block_rows(idx)
-    rng = np.random.default_rng(3)
-    X = rng.standard_normal((inf["ncols"], a.k)).astype(np.float32)
-    # calibrate on two block rows per thread, then size the sample to the
-    # target time: a multiple of the thread count, at least four block rows
-    # per thread (block rows are the unit the workers take), so that every
-    # thread stays busy
-    bc = int(min(nb, 2 * nthreads))
-    t = time.perf_counter()
-    oracle.spmm(idx, mat, X, nthreads=nthreads, brows=(0, bc))
-    dt = max(time.perf_counter() - t, 1e-4) / bc
-    b1 = int(target_s / dt) // nthreads * nthreads
-    b1 = int(min(nb, max(4 * nthreads, b1)))
-    nnz_s = oracle.block_rows_nnz(idx, mat, 0, b1)
+    return oracle
+
+
+def oracle_image(a):
+    """The bench workload's 2D image made by the oracle alone: its own R-MAT
+    stream (the same edges as the library's generator) and its own builder
+    (the restatement of matrix/fm_utils.cpp:228-433,617-715), so that no GPU
+    library is loaded in the process."""
+    oracle = oracle_mod()
+    src, dst = oracle.rmat_edges(a.scale, seed=1, permute=not a.no_permute)
+    vals = None
+    if a.weighted:
+        rng = np.random.default_rng(7)
+        vals = (1.0 - rng.random(len(src), dtype=np.float32)).astype(np.float32)  # (0, 1]
+    n = 1 << a.scale
+    idx, mat = oracle.build_image(src, dst, vals, nrows=n, ncols=n, block=(a.block, a.block), dedup=True)
+    return idx, mat
+
+
+def cpu_spmm_times(idx, mat, X, nthreads, runs, brows=None, Y=None):
+    """Wall times of `runs` oracle SpMMs (each as the reference's
+    sparse_matrix::multiply runs it: block-row tasks pulled by `nthreads`
+    workers, per-task copy of the tiles, thread-local output band copied into
+    Y) into one preallocated, already touched Y."""
+    oracle = oracle_mod()
+    h = oracle.header(idx)
+    if Y is None:
+        Y = np.zeros((h["nrows"], X.shape[1]), dtype=X.dtype)
+        Y.fill(0)
     times = []
-    for _ in range(reps or 1):
+    for _ in range(runs):
         t = time.perf_counter()
-        oracle.spmm(idx, mat, X, nthreads=nthreads, brows=(0, b1))
+        oracle.spmm(idx, mat, X, nthreads=nthreads, brows=brows, out=Y)
         times.append(time.perf_counter() - t)
-    full = b_alg(inf["nrows"], inf["ncols"], inf["nnz"], a.k, a.weighted)
-    per_nnz = full / inf["nnz"]
-    gbs = [per_nnz * nnz_s / x / 1e9 for x in times]
-    sample = (f"block rows [0,{b1}) of {nb} ({nnz_s} of {inf['nnz']} non-zeros, "
-              f"{a.block}x{a.block} tiles), FP32 k={a.k}, {nthreads} threads, "
-              f"GB/s = B_alg per nnz x sample nnz / time")
-    return gbs, sample, times
+    return times, Y
+
+
+def cpu_plan(idx, mat, X, nthreads, steps, budget_s):
+    """How much of the matrix one CPU step covers: the whole matrix when
+    `steps` whole-matrix SpMMs fit in `budget_s` seconds, else the first block
+    rows that do (a multiple of the thread count, at least four block rows
+    per thread).  Returns (brows or None, nnz covered, one calibration time)."""
+    oracle = oracle_mod()
+    nb = oracle.num_block_rows(idx)
+    nnz = oracle.block_rows_nnz(idx, mat, 0, nb)
+    (t_full,), Y = cpu_spmm_times(idx, mat, X, nthreads, 1)
+    if t_full * steps <= budget_s:
+        return None, nnz, t_full, Y
+    per = budget_s / steps
+    b1 = int(nb * per / t_full) // nthreads * nthreads
+    b1 = int(min(nb, max(4 * nthreads, b1)))
+    return (0, b1), oracle.block_rows_nnz(idx, mat, 0, b1), t_full, Y
+
+
+def cpu_workload_x(a, ncols):
+    rng = np.random.default_rng(3)
+    return rng.standard_normal((ncols, a.k)).astype(np.float32)
+
+
+def cpu_sample_desc(a, brows, nnz_s, nnz, nb, nthreads, model):
+    what = (f"the whole matrix ({nb} block rows, {nnz} non-zeros)" if brows is None else
+            f"block rows [0,{brows[1]}) of {nb} ({nnz_s} of {nnz} non-zeros)")
+    return (f"{what}, {a.block}x{a.block} tiles, FP32 k={a.k}, {nthreads} threads, sequential order, "
+            f"cpu_cache_size 1 MiB, per-task tile copy; GB/s = B_alg per nnz x nnz covered / time; CPU: {model}")
+
+
+def cpu_config_s16(nthreads, reps=5):
+    """The reference's CPU configuration: R-MAT scale 16 (edge factor 16,
+    seed 1, deduplicated, no self-loops, unweighted) times FP64 X (uniform in
+    [-1, 1]) with k in {1, 8}; tiles 16384^2 and 32768^2; sequential and
+    Hilbert order (matrix/sparse_matrix.cpp:120-186, matrix_config.h:88);
+    median of `reps` timed SpMMs after one warm-up, on `nthreads` threads."""
+    oracle = oracle_mod()
+    n = 1 << 16
+    src, dst = oracle.rmat_edges(16, seed=1)
+    rng = np.random.default_rng(11)
+    out = {"workload": "rmat-s16-ef16-unweighted, X FP64 uniform[-1,1]", "threads": nthreads,
+           "timing": f"median of {reps} after 1 warm-up, oracle (C restatement of the reference's CPU SpMM)"}
+    for tile in (16384, 32768):
+        idx, mat = oracle.build_image(src, dst, None, nrows=n, ncols=n, block=(tile, tile), dedup=True)
+        nnz = oracle.block_rows_nnz(idx, mat, 0, oracle.num_block_rows(idx))
+        for k in (1, 8):
+            X = rng.uniform(-1.0, 1.0, (n, k))
+            Y = np.zeros((n, k))
+            for order in ("seq", "hilbert"):
+                times = []
+                for i in range(reps + 1):
+                    t = time.perf_counter()
+                    oracle.spmm(idx, mat, X, nthreads=nthreads, hilbert=order == "hilbert", out=Y)
+                    if i:
+                        times.append(time.perf_counter() - t)
+                ms = float(np.median(times)) * 1e3
+                out[f"tile{tile}_k{k}_{order}"] = {"ms": round(ms, 4), "nnz": int(nnz),
+                                                   "gbs": round(b_alg(n, n, nnz, k, False, 8) / ms / 1e6, 3)}
+    return out
 
 
 class ClockSampler:
@@ -468,30 +535,58 @@ def large_run(a):
     return out
 
 
+def repo_libraries():
+    """The repository's shared libraries mapped into this process."""
+    libs = set()
+    try:
+        with open("/proc/self/maps") as f:
+            for line in f:
+                path = line.split()[-1] if len(line.split()) >= 6 else ""
+                if path.startswith(ROOT) and ".so" in path:
+                    libs.add(os.path.relpath(path, ROOT))
+    except OSError:
+        pass
+    return sorted(libs)
+
+
 def run_reference(a, rank, world):
+    """The reference arm: FlashMatrix's CPU SpMM (the oracle's restatement of
+    sparse_matrix::multiply over the 2D image, matrix/sparse_matrix.h:219-375,
+    sparse_matrix.cpp:251-473) on all host cores, on the same workload as the
+    GPU arm.  Only the oracle is loaded: its own R-MAT stream and builder make
+    the image.  Each step is one whole-matrix SpMM when --steps + --warmup of
+    them fit in about four minutes, else the first block rows that do."""
     if rank != 0:
         return
-    img, build_s = build_graph(a)
+    oracle = oracle_mod()
     nthreads, model = cpu_info()
-    inf = img.info()
-    # each step is a bounded sample of the workload: the whole run (warm-up
-    # included) holds about 90 s of CPU work, at least four block rows per
-    # host thread per step
-    warm = a.warmup
-    per = min(0.5, 90.0 / max(a.steps + warm, 1))
-    gbs, sample, times = cpu_sample(img, a, nthreads, per, reps=a.steps + warm)
-    gbs, times = gbs[warm:], times[warm:]
+    t0 = time.time()
+    idx, mat = oracle_image(a)
+    build_s = time.time() - t0
+    h = oracle.header(idx)
+    nb = oracle.num_block_rows(idx)
+    X = cpu_workload_x(a, h["ncols"])
+    runs = a.steps + a.warmup
+    brows, nnz_s, t_cal, Y = cpu_plan(idx, mat, X, nthreads, runs, 240.0)
+    nnz = oracle.block_rows_nnz(idx, mat, 0, nb)
+    times, _ = cpu_spmm_times(idx, mat, X, nthreads, runs, brows=brows, Y=Y)
+    times = times[a.warmup:]
+    per_nnz = b_alg(h["nrows"], h["ncols"], nnz, a.k, a.weighted) / nnz
+    gbs = [per_nnz * nnz_s / t / 1e9 for t in times]
     value = float(np.median(gbs))
+    sample = cpu_sample_desc(a, brows, nnz_s, nnz, nb, nthreads, model)
     line = {
         "metric": "SpMM GB/s (algorithmic bytes / time)", "value": round(value, 3), "unit": "GB/s",
-        "impl": "reference", "n_gpus": world, "steps": a.steps, "warmup": warm,
+        "impl": "reference", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": round(float(np.median(times)) * 1e3, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": workload_name(a), "scale": a.scale, "k": a.k, "nnz": inf["nnz"],
-                   "block": a.block, "sample": sample},
+        "config": {"workload": workload_name(a), "scale": a.scale, "k": a.k, "nnz": nnz,
+                   "block": a.block, "whole_matrix_per_step": brows is None, "sample": sample,
+                   "oracle_build_s": round(build_s, 2)},
         "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": nthreads, "kind": "port",
-                         "sample": sample + f"; CPU: {model}"},
+                         "sample": sample, "cpu_config": cpu_config_s16(nthreads)},
         "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "repo_libraries_loaded": repo_libraries(),
     }
     print(json.dumps(line), flush=True)
 
@@ -605,9 +700,19 @@ def main():
     cpu = None
     if cpu_img is not None:
         nthreads, model = cpu_info()
-        gbs, sample, _ = cpu_sample(cpu_img, a, nthreads, a.cpu_seconds)
-        cpu = {"value": round(gbs[0], 3), "unit": "GB/s", "cores": nthreads, "kind": "port",
-               "sample": sample + f"; CPU: {model}"}
+        cidx, cmat = cpu_img.bytes()
+        oracle = oracle_mod()
+        nb = oracle.num_block_rows(cidx)
+        Xc = cpu_workload_x(a, n_cols)
+        # whole-matrix SpMMs totalling about --cpu-seconds (at least 3)
+        brows, nnz_s, t_cal, Yc = cpu_plan(cidx, cmat, Xc, nthreads, 3, max(a.cpu_seconds, 3.0))
+        reps = max(3, min(9, int(a.cpu_seconds / max(t_cal, 1e-3))))
+        times, _ = cpu_spmm_times(cidx, cmat, Xc, nthreads, reps, brows=brows, Y=Yc)
+        del Xc, Yc
+        gbs = per_spmm / nnz * nnz_s / float(np.median(times)) / 1e9
+        cpu = {"value": round(gbs, 3), "unit": "GB/s", "cores": nthreads, "kind": "port",
+               "sample": cpu_sample_desc(a, brows, nnz_s, nnz, nb, nthreads, model) + f"; median of {reps}",
+               "cpu_config": cpu_config_s16(nthreads)}
 
     eig = prk = None
     if rank == 0 and not a.skip_eigen:

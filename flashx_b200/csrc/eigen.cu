@@ -1010,6 +1010,7 @@ int fmx_eigen_solve(const fmx_matrix *m, const float *row_scale, const fmx_eigen
 {
 	if (!m || !opt) return set_error(FMX_ERR_INVAL, "null matrix or options");
 	device_guard on_device(matrix_device(m));
+	if (!on_device.ok()) return set_error(FMX_ERR_CUDA, "cannot make the matrix's device %d current", matrix_device(m));
 	uint64_t nrows = 0, ncols = 0, nnz = 0;
 	int prim = 0;
 	E_TRY(fmx_matrix_info(m, &nrows, &ncols, &nnz, &prim, nullptr));
@@ -1050,6 +1051,7 @@ int fmx_na_scale(const fmx_matrix *m, float *s, void *stream)
 {
 	if (!m || !s) return set_error(FMX_ERR_INVAL, "null argument");
 	device_guard on_device(matrix_device(m));
+	if (!on_device.ok()) return set_error(FMX_ERR_CUDA, "cannot make the matrix's device %d current", matrix_device(m));
 	uint64_t nrows = 0, ncols = 0, nnz = 0;
 	int prim = 0;
 	E_TRY(fmx_matrix_info(m, &nrows, &ncols, &nnz, &prim, nullptr));

@@ -100,14 +100,22 @@ cudaError_t work_alloc(void **p, size_t bytes, cudaStream_t st);
 
 // The device a matrix lives on.
 int matrix_device(const fmx_matrix *m);
-// Makes `device` current for its lifetime and then restores the caller's.
+// Makes `device` current for its lifetime and then restores the caller's;
+// ok() is false when `device` could not be made current.
 struct device_guard {
 	int prev = -1;
+	bool ok_ = true;
 	explicit device_guard(int device)
 	{
 		int cur = 0;
-		if (cudaGetDevice(&cur) == cudaSuccess && cur != device && cudaSetDevice(device) == cudaSuccess) prev = cur;
+		if (cudaGetDevice(&cur) != cudaSuccess) {
+			ok_ = false;
+		} else if (cur != device) {
+			if (cudaSetDevice(device) == cudaSuccess) prev = cur;
+			else ok_ = false;
+		}
 	}
+	bool ok() const { return ok_; }
 	~device_guard()
 	{
 		if (prev >= 0) cudaSetDevice(prev);

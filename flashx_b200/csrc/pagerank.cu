@@ -86,6 +86,7 @@ int fmx_pagerank(const fmx_matrix *m, uint64_t max_iters, float damping, float *
 {
 	if (!m || !pr) return set_error(FMX_ERR_INVAL, "null argument");
 	device_guard on_device(matrix_device(m));    // before the buffers: freed on the matrix's device
+	if (!on_device.ok()) return set_error(FMX_ERR_CUDA, "cannot make the matrix's device %d current", matrix_device(m));
 	uint64_t nr = 0, nc = 0, nz = 0;
 	int prim = 0;
 	P_TRY(fmx_matrix_info(m, &nr, &nc, &nz, &prim, nullptr));

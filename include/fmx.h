@@ -212,12 +212,17 @@ int fmx_spmm(const fmx_matrix *m, int x_type, const void *X, int64_t ldx,
  * fmx_spmm with x_type = y_type = FMX_F32 and no row scales, for binary or
  * float-weighted matrices.  Its scratch is one fixed 32 MiB array compiled
  * into libfmx, present on every GPU that loads the library until the process
- * exits; matrices whose SpMM scratch (fmx_matrix_hot) exceeds 32 MiB are
- * rejected with FMX_ERR_UNSUPPORTED.  The first call on a device looks up the
- * array's device address (cudaGetSymbolAddress), so make that first call
- * before any stream capture.  All calls share the array: calls that overlap on
- * the GPU (on different streams, or from different threads) race and must not
- * be issued. */
+ * exits.  A matrix needs H + 1024 * P bytes of it, where H is
+ * (n_hot_cols + 1) * 128 rounded up to a multiple of 256 and P the number of
+ * chunk-sum slots (from fmx_matrix_hot: P = (scratch_bytes - (n_hot_cols + 1)
+ * * 128) / 2048); matrices that need more than 32 MiB are rejected with
+ * FMX_ERR_UNSUPPORTED.  The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress) and keeps it for the life of the
+ * process, so make that first call before any stream capture; a device reset
+ * (cudaDeviceReset) while the library is loaded is not supported by this
+ * entry point.  All calls share the array: calls that overlap on the GPU (on
+ * different streams, or from different threads) race and must not be
+ * issued. */
 int fmx_spmm_noalloc(const fmx_matrix *m, const float *X, int64_t ldx, float *Y,
                      int64_t ldy, int64_t k, void *stream);
 

@@ -40,6 +40,7 @@
 #include <string.h>
 #include <stdio.h>
 #include <time.h>
+#include <unistd.h>
 
 #define ORC_PAGE 4096
 #define ORC_MAGIC 0x123456789FFFFFFLL
@@ -93,14 +94,85 @@ static int ilog2u(uint64_t v) { int l = 0; while ((1ULL << l) < v) l++; return l
 
 typedef struct { uint32_t r, c; uint64_t i; } orc_edge;
 
-static int cmp_edge(const void *a, const void *b)
+/*
+ * The edges in (row, column) order, equal keys in input order: std::sort by
+ * (row, column) (fm_utils.cpp:469,521) with duplicates resolved the way
+ * std::unique keeps them, as the first occurrence in the input.  A stable
+ * LSD radix sort over the key bits gives exactly that order; it runs its
+ * passes on `nth` threads (per-thread digit counts, thread-ordered scatter,
+ * so each pass stays stable).
+ */
+#define ORC_RADIX_BITS 11
+typedef struct {
+	orc_edge *from, *to;
+	uint64_t n, b0, b1;
+	int shift, cbits, nth, t;
+	uint64_t *cnt;      /* [nth][1 << ORC_RADIX_BITS] */
+	pthread_barrier_t *bar;
+} orc_rs_arg;
+
+static inline uint32_t orc_digit(const orc_edge *e, int shift, int cbits)
 {
-	const orc_edge *x = a, *y = b;
-	if (x->r != y->r) return x->r < y->r ? -1 : 1;
-	if (x->c != y->c) return x->c < y->c ? -1 : 1;
-	/* std::sort is not stable; ties only matter for duplicates whose first
-	 * occurrence std::unique keeps.  Keep input order among equal keys. */
-	return x->i < y->i ? -1 : (x->i > y->i);
+	const uint64_t key = ((uint64_t)e->r << cbits) | e->c;
+	return (uint32_t)(key >> shift) & ((1u << ORC_RADIX_BITS) - 1);
+}
+
+static void *orc_rs_worker(void *p)
+{
+	orc_rs_arg *a = p;
+	const uint32_t nb = 1u << ORC_RADIX_BITS;
+	uint64_t *mine = a->cnt + (uint64_t)a->t * nb;
+	memset(mine, 0, sizeof(uint64_t) * nb);
+	for (uint64_t i = a->b0; i < a->b1; i++) mine[orc_digit(&a->from[i], a->shift, a->cbits)]++;
+	pthread_barrier_wait(a->bar);
+	if (a->t == 0) {
+		/* exclusive offsets in (digit, thread) order */
+		uint64_t s = 0;
+		for (uint32_t d = 0; d < nb; d++)
+			for (int t = 0; t < a->nth; t++) {
+				uint64_t c = a->cnt[(uint64_t)t * nb + d];
+				a->cnt[(uint64_t)t * nb + d] = s;
+				s += c;
+			}
+	}
+	pthread_barrier_wait(a->bar);
+	for (uint64_t i = a->b0; i < a->b1; i++) a->to[mine[orc_digit(&a->from[i], a->shift, a->cbits)]++] = a->from[i];
+	return NULL;
+}
+
+static int orc_sort_edges(orc_edge *e, uint64_t m, uint64_t nrows, uint64_t ncols)
+{
+	if (m < 2) return 0;
+	const int rbits = ilog2u(nrows), cbits = ilog2u(ncols);
+	const int bits = rbits + cbits;
+	orc_edge *tmp = malloc(sizeof(orc_edge) * m);
+	if (!tmp) return -1;
+	long ncpu = sysconf(_SC_NPROCESSORS_ONLN);
+	int nth = (int)(m / (1u << 20));
+	if (nth > ncpu) nth = (int)ncpu;
+	if (nth > 64) nth = 64;
+	if (nth < 1) nth = 1;
+	uint64_t *cnt = malloc(sizeof(uint64_t) * (uint64_t)nth << ORC_RADIX_BITS);
+	pthread_t th[64];
+	orc_rs_arg args[64];
+	pthread_barrier_t bar;
+	pthread_barrier_init(&bar, NULL, (unsigned)nth);
+	orc_edge *from = e, *to = tmp;
+	for (int shift = 0; shift < bits; shift += ORC_RADIX_BITS) {
+		for (int t = 0; t < nth; t++) {
+			args[t] = (orc_rs_arg){from, to, m, m * (uint64_t)t / (uint64_t)nth, m * (uint64_t)(t + 1) / (uint64_t)nth,
+					shift, cbits, nth, t, cnt, &bar};
+			if (t) pthread_create(&th[t], NULL, orc_rs_worker, &args[t]);
+		}
+		orc_rs_worker(&args[0]);
+		for (int t = 1; t < nth; t++) pthread_join(th[t], NULL);
+		orc_edge *x = from; from = to; to = x;
+	}
+	pthread_barrier_destroy(&bar);
+	if (from != e) memcpy(e, from, sizeof(orc_edge) * m);
+	free(cnt);
+	free(tmp);
+	return 0;
 }
 
 /*
@@ -148,7 +220,7 @@ int orc_build_image(const uint32_t *src, const uint32_t *dst, const void *vals,
 		if (!keep_self && src[i] == dst[i]) continue;
 		e[m].r = src[i]; e[m].c = dst[i]; e[m].i = i; m++;
 	}
-	qsort(e, m, sizeof(orc_edge), cmp_edge);
+	if (orc_sort_edges(e, m, nrows, ncols)) { free(e); return -1; }
 	if (dedup && m) {
 		uint64_t w = 1;
 		for (uint64_t i = 1; i < m; i++)
@@ -759,6 +831,107 @@ double orc_now(void)
 	struct timespec ts;
 	clock_gettime(CLOCK_MONOTONIC, &ts);
 	return ts.tv_sec + ts.tv_nsec * 1e-9;
+}
+
+/* ------------------------------------------------------------------------
+ * The synthetic R-MAT workload (test infrastructure)
+ *
+ * The benchmark graphs are R-MAT graphs with FlashX's quadrant probabilities
+ * (flash-graph/tools/rmat-gen.cpp:43-44).  The reference draws them with
+ * Boost.Graph's rmat_iterator, which is not in the tree; both arms of the
+ * benchmark instead use one counter-based stream: edge e depends only on
+ * (seed, e).  This is a second implementation of that stream, so that the
+ * CPU arm never loads the GPU library; tests/test_oracle_pin.py checks that
+ * it yields the same edges as the library's generator.
+ *   per edge: h0 = mix(key ^ e * 0xD6E8FEB86659FD93); for each of the
+ *   `scale` levels one 32-bit draw u (two per mix of h0 + l * golden), row
+ *   bit = u >= a + b, column bit = a <= u < a + b or u >= a + b + c (both
+ *   as fractions of 2^32), most significant bit first; then, with permute,
+ *   both ids go through a seeded bijection of [0, 2^scale): four rounds of
+ *   x = (x * odd + add) mod 2^scale, x ^= x >> (scale / 2 + 1).
+ * ------------------------------------------------------------------------ */
+static uint64_t orc_mix64(uint64_t z)
+{
+	/* splitmix64's finaliser (Steele, Lea and Flood, 2014) */
+	z += 0x9E3779B97F4A7C15ULL;
+	z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+	z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+	return z ^ (z >> 31);
+}
+
+typedef struct {
+	uint64_t key;
+	uint32_t ta, tab, tabc;
+	int scale, permute;
+	uint64_t mul[4], add[4];
+	uint32_t *src, *dst;
+	uint64_t e0, e1;
+} orc_rmat_job;
+
+static uint32_t orc_rmat_relabel(const orc_rmat_job *p, uint32_t v)
+{
+	const uint64_t mask = (1ULL << p->scale) - 1;
+	const int sh = p->scale / 2 + 1;
+	uint64_t x = v;
+	for (int r = 0; r < 4; r++) {
+		x = (x * p->mul[r] + p->add[r]) & mask;
+		x ^= x >> sh;
+	}
+	return (uint32_t)x;
+}
+
+static void *orc_rmat_worker(void *arg)
+{
+	orc_rmat_job *p = arg;
+	for (uint64_t e = p->e0; e < p->e1; e++) {
+		const uint64_t h0 = orc_mix64(p->key ^ (e * 0xD6E8FEB86659FD93ULL));
+		uint32_t r = 0, c = 0;
+		uint64_t h = 0;
+		for (int l = 0; l < p->scale; l++) {
+			if ((l & 1) == 0) h = orc_mix64(h0 + (uint64_t)l * 0x9E3779B97F4A7C15ULL);
+			const uint32_t u = (l & 1) ? (uint32_t)(h >> 32) : (uint32_t)h;
+			r = (r << 1) | (uint32_t)(u >= p->tab);
+			c = (c << 1) | (uint32_t)((u >= p->ta && u < p->tab) || u >= p->tabc);
+		}
+		if (p->permute) { r = orc_rmat_relabel(p, r); c = orc_rmat_relabel(p, c); }
+		p->src[e] = r;
+		p->dst[e] = c;
+	}
+	return NULL;
+}
+
+/* nedges R-MAT edges of 2^scale vertices into src/dst.  Returns 0 or -1. */
+int orc_rmat_edges(int scale, uint64_t nedges, double a, double b, double c, uint64_t seed, int permute,
+		uint32_t *src, uint32_t *dst, int nthreads)
+{
+	if (scale < 1 || scale > 31 || !(a >= 0 && b >= 0 && c >= 0 && a + b + c <= 1.0)) return -1;
+	orc_rmat_job p;
+	memset(&p, 0, sizeof(p));
+	#define ORC_TH(x) ((x) * 4294967296.0 >= 4294967295.0 ? 0xFFFFFFFFu : (uint32_t)((x) * 4294967296.0))
+	p.key = orc_mix64(seed ^ 0x5851F42D4C957F2DULL);
+	p.ta = ORC_TH(a); p.tab = ORC_TH(a + b); p.tabc = ORC_TH(a + b + c);
+	#undef ORC_TH
+	p.scale = scale; p.permute = permute;
+	uint64_t s = orc_mix64(seed + 0x1234567ULL);
+	for (int r = 0; r < 4; r++) {
+		s = orc_mix64(s); p.mul[r] = s | 1ULL;
+		s = orc_mix64(s); p.add[r] = s;
+	}
+	p.src = src; p.dst = dst;
+	if (nthreads < 1) nthreads = (int)sysconf(_SC_NPROCESSORS_ONLN);
+	if (nthreads > 256) nthreads = 256;
+	if (nthreads < 1) nthreads = 1;
+	orc_rmat_job jobs[256];
+	pthread_t th[256];
+	for (int t = 0; t < nthreads; t++) {
+		jobs[t] = p;
+		jobs[t].e0 = nedges * (uint64_t)t / (uint64_t)nthreads;
+		jobs[t].e1 = nedges * (uint64_t)(t + 1) / (uint64_t)nthreads;
+		if (t) pthread_create(&th[t], NULL, orc_rmat_worker, &jobs[t]);
+	}
+	orc_rmat_worker(&jobs[0]);
+	for (int t = 1; t < nthreads; t++) pthread_join(th[t], NULL);
+	return 0;
 }
 
 /* ------------------------------------------------------------------------

@@ -21,7 +21,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "liboracle.so")
 REFWALK_SO = os.path.join(HERE, "_ref", "libfmx_refwalk.so")
 REFFG_SO = os.path.join(HERE, "_ref", "libfmx_reffg.so")
-REFERENCE_TREE = "/root/reference"
+# Where the FlashX source tree lies, for building the reference walkers
+# (`make ref`); unset means "not available" and the walkers are not built.
+REFERENCE_TREE = os.environ.get("FMX_REFERENCE_TREE") or None
 
 D_F32, D_F64, D_I32, D_I64 = 0, 1, 3, 4
 P_BOOL, P_INTEGER, P_LONG, P_FLOAT, P_DOUBLE = 0, 4, 6, 8, 9
@@ -29,13 +31,18 @@ _NP = {D_F32: np.float32, D_F64: np.float64, D_I32: np.int32, D_I64: np.int64}
 _D_OF = {np.dtype(v): k for k, v in _NP.items()}
 
 
-def build(ref=None):
-    """Compile the oracle (and the reference walker when the tree exists)."""
+def build(ref=None, tree=None):
+    """Compile the oracle, and the reference walkers when the FlashX tree is
+    given (`tree`, else the FMX_REFERENCE_TREE environment variable) and
+    holds matrix/."""
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
+    tree = tree or REFERENCE_TREE
     if ref is None:
-        ref = os.path.isdir(os.path.join(REFERENCE_TREE, "matrix"))
+        ref = bool(tree) and os.path.isdir(os.path.join(tree, "matrix"))
     if ref:
-        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REFERENCE_TREE}"], check=True)
+        if not tree:
+            raise ValueError("building the reference walkers needs the FlashX tree (FMX_REFERENCE_TREE)")
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={tree}"], check=True)
 
 
 _orc = None
@@ -68,6 +75,8 @@ def orc():
         L.orc_hilbert_xy2d.restype = i32
         L.orc_hilbert_xy2d.argtypes = [i32, i32, i32]
         L.orc_now.restype = C.c_double
+        L.orc_rmat_edges.restype = i32
+        L.orc_rmat_edges.argtypes = [i32, u64, C.c_double, C.c_double, C.c_double, u64, i32, vp, vp, i32]
         L.orc_fg_build.restype = i32
         L.orc_fg_build.argtypes = [vp, vp, vp, C.c_uint32, u64, u64, i32, C.POINTER(vp), C.POINTER(u64)]
         L.orc_fg_spmm.restype = i32
@@ -149,14 +158,22 @@ def header(idx):
     return dict(nrows=nrows, ncols=ncols, entry_size=esize, prim=prim, block_h=bh, block_w=bw)
 
 
-def spmm(idx, mat, X, nthreads=1, hilbert=False, cpu_cache_size=0, copy_task=True, brows=None):
-    """Oracle SpMM Y = A X (X: 2-D numpy array, ncols x k, row-major)."""
+def spmm(idx, mat, X, nthreads=1, hilbert=False, cpu_cache_size=0, copy_task=True, brows=None, out=None):
+    """Oracle SpMM Y = A X (X: 2-D numpy array, ncols x k, row-major).
+
+    `out`, when given, is the C-contiguous nrows x k result array of X's
+    dtype (rows outside `brows` are left as they are)."""
     X = np.ascontiguousarray(X)
     if X.ndim == 1:
         X = X[:, None]
     d = _D_OF[X.dtype]
     h = header(idx)
-    Y = np.zeros((h["nrows"], X.shape[1]), dtype=X.dtype)
+    if out is not None:
+        if out.shape != (h["nrows"], X.shape[1]) or out.dtype != X.dtype or not out.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous nrows x k array of X's dtype")
+        Y = out
+    else:
+        Y = np.zeros((h["nrows"], X.shape[1]), dtype=X.dtype)
     b0, b1 = (0, 0) if brows is None else brows
     rc = orc().orc_spmm(idx, len(idx), mat, len(mat), d, X.ctypes.data, Y.ctypes.data, X.shape[1],
                         nthreads, int(hilbert), cpu_cache_size, int(copy_task), b0, b1)
@@ -205,6 +222,18 @@ def pagerank(idx, mat, t_idx, t_mat, max_iters=30, damping=0.85, nthreads=1):
     if rc:
         raise ValueError("oracle PageRank failed")
     return pr, it.value
+
+
+def rmat_edges(scale, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=1, permute=True, nedges=None, nthreads=0):
+    """The benchmark's R-MAT edge stream (uint32 src, dst), generated on the
+    CPU without the GPU library: the same edges as
+    flashx_b200.graphs.rmat_edges for the same arguments."""
+    m = int(nedges if nedges is not None else edge_factor * (1 << scale))
+    src = np.empty(m, dtype=np.uint32)
+    dst = np.empty(m, dtype=np.uint32)
+    if orc().orc_rmat_edges(scale, m, a, b, c, seed, int(permute), src.ctypes.data, dst.ctypes.data, nthreads):
+        raise ValueError("oracle R-MAT: bad arguments")
+    return src, dst
 
 
 def num_block_rows(idx):

@@ -63,3 +63,24 @@ def test_reference_arm_other_ranks_exit_without_work():
                        env=env, capture_output=True, text=True, timeout=120)
     assert r.returncode == 0
     assert r.stdout.strip() == ""
+
+
+def test_reference_arm_loads_only_the_oracle():
+    """Rank 0 of the reference arm times the whole matrix per step in a
+    process that maps no library of the GPU path: the oracle's own R-MAT
+    stream and builder make the image."""
+    import json
+    env = dict(os.environ, RANK="0", WORLD_SIZE="1", LOCAL_RANK="0")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--scale", "14",
+                        "--steps", "2", "--warmup", "1"], env=env, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference"
+    assert line["repo_libraries_loaded"] == ["oracle/_build/liboracle.so"]
+    assert line["config"]["whole_matrix_per_step"] is True
+    assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
+    cfg = line["cpu_baseline"]["cpu_config"]
+    for tile in (16384, 32768):
+        for k in (1, 8):
+            for order in ("seq", "hilbert"):
+                assert cfg[f"tile{tile}_k{k}_{order}"]["gbs"] > 0

@@ -8,6 +8,8 @@
    make_golden.py with the reference walker).
 3. Against the known answer of matrix/test/rand_mat_gen.cpp:178-199.
 4. Hilbert order against matrix/hilbert_curve.cpp.
+5. The oracle's R-MAT stream against the library's generator (the CPU arm
+   of the benchmark makes its workload without the GPU library).
 """
 import hashlib
 import os
@@ -150,3 +152,25 @@ def test_oracle_pagerank_matches_restatement():
         np.add.at(out, c.astype(np.int64), x[r.astype(np.int64)].astype(np.float64))
         p = (out.astype(np.float32) * np.float32(0.85) + teleport).astype(np.float32)
     np.testing.assert_allclose(pr, p, rtol=1e-5, atol=1e-9)
+
+
+@pytest.mark.parametrize("scale,seed,permute", [(8, 1, True), (14, 1, True), (12, 3, False), (17, 9, True)])
+def test_oracle_rmat_stream_matches_the_library(scale, seed, permute):
+    from flashx_b200.graphs import rmat_edges
+    a = rmat_edges(scale, seed=seed, permute=permute)
+    b = oracle.rmat_edges(scale, seed=seed, permute=permute, nthreads=3)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+
+
+def test_oracle_builder_sort_keeps_first_duplicates():
+    """The builder's parallel radix sort: duplicates keep the first
+    occurrence's value, exactly as the library's builder does."""
+    from flashx_b200 import matrix_image
+    rng = np.random.default_rng(8)
+    n, m = 3000, 3_000_000            # several sort threads, many duplicates
+    src = rng.integers(0, n, m).astype(np.uint32)
+    dst = rng.integers(0, n, m).astype(np.uint32)
+    vals = rng.standard_normal(m).astype(np.float32)
+    idx, mat = oracle.build_image(src, dst, vals, nrows=n, ncols=n, block=(1024, 512), dedup=True)
+    i2, m2 = matrix_image.build(src, dst, vals, nrows=n, ncols=n, block_size=(1024, 512), dedup=True).bytes()
+    assert bytes(idx) == bytes(i2) and bytes(mat) == bytes(m2)

@@ -5,12 +5,16 @@ It exists for callers that cannot allocate device memory while they run
 callbacks, on real-time paths).  It keeps its scratch in a fixed array
 compiled into libfmx.  These tests call it through the C ABI, twice in a
 row (the second call sees the first call's leftovers in the shared array),
-and compare with fmx_spmm within the parity tolerance of the other tests.
+and require results identical to fmx_spmm's bit for bit (the two run the
+same kernels in the same order) and to the CPU oracle's (bit for bit with
+integer-valued inputs, within the 1e-5 parity tolerance otherwise).
 
 This file is collected last on purpose, so that a run which stops at the
 first failure has already run every other test.
 """
 import ctypes as C
+import os
+import sys
 
 import numpy as np
 import pytest
@@ -18,9 +22,24 @@ import pytest
 from flashx_b200 import _lib, matrix_image, sparse_matrix
 from flashx_b200.graphs import rmat_edges
 
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle"))
+import oracle  # noqa: E402
+
 pytestmark = pytest.mark.gpu
 
 RTOL = 1e-5
+SCRATCH = 32 << 20
+
+
+def _scratch_need(m):
+    """The fixed-scratch bytes fmx_spmm_noalloc needs for this matrix: the
+    hot pack, (n_hot + 1) rows of 128 bytes rounded up to 256 bytes, plus
+    4-byte chunk sums, 256 per partial slot.  fmx_matrix_hot's scratch count
+    holds the partial slots at 8 bytes: (n_hot + 1) * 128 + slots * 2048."""
+    n_hot, _, scratch = m.hot()
+    hot = (n_hot + 1) * 128
+    slots = (scratch - hot) // 2048
+    return (hot + 255) // 256 * 256 + slots * 256 * 4
 
 
 def _noalloc(torch, m, x, y):
@@ -39,8 +58,7 @@ def test_noalloc_matches_fmx_spmm_twice(torch_cuda, weighted):
         vals = (1.0 - np.random.default_rng(1).random(len(src))).astype(np.float32)
     img = matrix_image.build(src, dst, vals, nrows=n, ncols=n, block_size=(16384, 16384), dedup=True)
     m = sparse_matrix.create(img, None)
-    hot_cols, _, scratch = m.hot()
-    assert scratch < 32 << 20
+    assert 0 < _scratch_need(m) <= SCRATCH
     g = torch.Generator(device="cuda").manual_seed(3)
     for k in (16, 1, 130, 32):
         x = torch.randn((n, k), generator=g, device="cuda")
@@ -50,8 +68,23 @@ def test_noalloc_matches_fmx_spmm_twice(torch_cuda, weighted):
             y = torch.full((n, k), float("nan"), device="cuda")
             assert _noalloc(torch, m, x, y) == _lib.FMX_OK, _lib.last_error()
             torch.cuda.synchronize()
-            np.testing.assert_allclose(y.cpu().numpy(), ref.cpu().numpy(), rtol=RTOL,
-                                       atol=RTOL * float(ref.abs().max()))
+            assert torch.equal(y, ref), f"k={k}: differs from fmx_spmm"
+    # against the CPU oracle: bit for bit for the binary matrix with
+    # integer-valued X (every sum exact), else within the parity tolerance
+    idx, mat = img.bytes()
+    xi = np.random.default_rng(4).integers(-8, 9, (n, 16)).astype(np.float32)
+    xf = np.random.default_rng(5).standard_normal((n, 16)).astype(np.float32)
+    for xh, exact in ((xi, not weighted), (xf, False)):
+        want = oracle.spmm(idx, mat, xh)
+        for _ in range(2):
+            y = torch.full((n, 16), float("nan"), device="cuda")
+            assert _noalloc(torch, m, torch.from_numpy(xh).cuda(), y) == _lib.FMX_OK, _lib.last_error()
+            torch.cuda.synchronize()
+            got = y.cpu().numpy()
+            if exact:
+                assert np.array_equal(got, want)
+            else:
+                np.testing.assert_allclose(got, want, rtol=RTOL, atol=RTOL * float(np.abs(want).max()))
 
 
 def test_noalloc_rejects_matrices_beyond_its_scratch(torch_cuda):
@@ -59,7 +92,7 @@ def test_noalloc_rejects_matrices_beyond_its_scratch(torch_cuda):
     n = 1 << 20
     src, dst = rmat_edges(20, seed=2)
     m = sparse_matrix.create(matrix_image.build(src, dst, None, nrows=n, ncols=n, dedup=True), None)
-    assert m.hot()[2] > 32 << 20
+    assert _scratch_need(m) > SCRATCH
     x = torch.zeros((n, 16), device="cuda")
     y = torch.zeros((n, 16), device="cuda")
     assert _noalloc(torch, m, x, y) == _lib.FMX_ERR_UNSUPPORTED
