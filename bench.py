@@ -319,6 +319,48 @@ def _timed_solve(torch, dev, fn, reps=5):
     return float(np.median(times)), res
 
 
+def eigenspace_errors(rows, cols, n, vals, X):
+    """Errors of computed eigenpairs of D^-1/2 A D^-1/2 (A symmetric, binary,
+    D = A 1) against the exact FP64 eigenspace of eigenvalue 1: for an
+    undirected graph it is span{D^1/2 1_C} over the connected components C
+    with edges, one dimension per component.  Per vector x_j (FP64 on the
+    host): sin of its angle to that space, ||x - P x|| / ||x||, and
+    |lambda_j - 1|; plus the largest principal angle between span(X) and
+    the space (X orthonormalised first).  `rows`, `cols`: the matrix's
+    non-zeros."""
+    import scipy.sparse as sp
+    from scipy.sparse.csgraph import connected_components
+    A = sp.csr_matrix((np.ones(len(rows), dtype=np.float32), (rows, cols)), shape=(n, n))
+    deg = np.asarray(A.sum(axis=1)).ravel().astype(np.float64)
+    ncomp, label = connected_components(A, directed=False)
+    del A
+    has = deg > 0
+    vol = np.bincount(label, weights=deg, minlength=ncomp)
+    sq = np.sqrt(deg)
+    X = np.asarray(X, dtype=np.float64)
+
+    def resid(Z):
+        # Z - P Z with P the orthogonal projector onto span{D^1/2 1_C}
+        out = np.empty_like(Z)
+        for j in range(Z.shape[1]):
+            s = np.bincount(label, weights=sq * Z[:, j], minlength=ncomp)
+            coef = np.divide(s, vol, out=np.zeros_like(s), where=vol > 0)
+            out[:, j] = Z[:, j] - sq * coef[label]
+        return out
+
+    R = resid(X)
+    sin_j = np.linalg.norm(R, axis=0) / np.maximum(np.linalg.norm(X, axis=0), 1e-300)
+    Q, _ = np.linalg.qr(X)
+    RQ = resid(Q)
+    s2 = np.linalg.eigvalsh(RQ.T @ RQ)
+    mult = int(np.unique(label[has]).size)
+    return {"eigenspace": f"eigenvalue 1 of D^-1/2 A D^-1/2: span{{D^1/2 1_C}}, {mult} components with edges",
+            "multiplicity_covers_block": mult >= X.shape[1],
+            "sin_angle_to_eigenspace": [float(f"{v:.3e}") for v in sin_j],
+            "abs_eigenvalue_error": [float(f"{abs(v - 1.0):.3e}") for v in vals],
+            "largest_principal_angle_sin": float(f"{np.sqrt(max(s2.max(), 0.0)):.3e}")}
+
+
 def _solve_summary(ms, r):
     return {"ms": round(ms, 2), "ms_each": list(getattr(_timed_solve, "last_times", [])),
             "spmm_calls": int(r.status.spmm_calls), "num_ops": int(r.status.num_ops),
@@ -342,10 +384,11 @@ def eigen_measure(a, dev):
     t0 = time.time()
     s, d = rmat_edges(a.eig_scale, seed=1)
     s, d = symmetrize(s, d)
-    m = sparse_matrix.create(matrix_image.build(s, d, None, nrows=n, ncols=n, block_size=(16384, 16384),
-                                                dedup=True), None, device=dev.index)
+    img = matrix_image.build(s, d, None, nrows=n, ncols=n, block_size=(16384, 16384), dedup=True)
+    m = sparse_matrix.create(img, None, device=dev.index)
     del s, d
     op = NA_operator(m, device=dev.index)
+    results = {}
     out = {"workload": f"rmat-s{a.eig_scale}-ef16-symmetrised-na-top8-block16-tol1e-6", "n": n,
            "nnz": int(m.get_nnz()), "build_s": round(time.time() - t0, 2),
            "timing": "median of 5 after 1 warm-up, CUDA events around the whole solve (host loop included)"}
@@ -353,6 +396,7 @@ def eigen_measure(a, dev):
         o = ws.eigen_opts(8, 1e-6, prec)
         ms, r = _timed_solve(torch, dev, lambda: compute_eigen(op, True, o))
         out[prec] = _solve_summary(ms, r)
+        results[prec] = r
     out["speedup_mixed_vs_plain"] = round(out["plain"]["ms"] / out["mixed"]["ms"], 3)
     weights = os.path.join(ROOT, "flashx_b200", "warmstart_weights.f32")
     if not os.path.exists(weights):
@@ -364,7 +408,17 @@ def eigen_measure(a, dev):
     out["mixed_learned"] = _solve_summary(ms, r)
     out["mixed_learned"]["spmm_calls"] += ws.SPMM_PER_START
     out["speedup_learned_mixed_vs_plain"] = round(out["plain"]["ms"] / ms, 3)
-    del op, m
+    results["mixed_learned"] = r
+    # per-pair errors against the exact FP64 eigenspace (computed on the host)
+    oracle = oracle_mod()
+    idx, mat = img.bytes()
+    rows, cols = oracle.nonzeros(idx, mat)
+    del img, idx, mat
+    for name, res in results.items():
+        e = eigenspace_errors(rows, cols, n, res.vals, res.vecs.cpu().numpy())
+        e["residual"] = [float(f"{v:.3e}") for v in res.residuals]
+        out[name]["errors"] = e
+    del rows, cols, results, op, m
     rows = []
     for i in range(a.eig_sbm):
         inst = ws.sbm_instance(30_000_000 + i, solve=False)
