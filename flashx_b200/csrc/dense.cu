@@ -308,6 +308,407 @@ tc_gemm_kernel(const float *__restrict__ X, int64_t ldx, int K, const float *__r
 }
 
 // ---------------------------------------------------------------------------
+// Pipelined tensor-core kernels: Y = X B (GEMM) and part[cta] = X^T W (Gram).
+//
+// Rows of X (and W) stream through shared memory in tiles of 128 rows, one
+// cp.async.bulk copy per tile and matrix (rows of ldx floats, contiguous).
+// Warp roles (320 threads, one CTA per SM):
+//   warp 0     producer: the bulk copies, into a ring of RS raw stages
+//   warp 1     MMA issuer (one lane) and TMEM owner
+//   warps 2-5  converters (thread r owns row r of a tile): raw rows -> MMA
+//              operands in a ring of OS operand stages; 3xTF32 splits
+//              x = hi + lo (hi = x with the low 13 mantissa bits cleared,
+//              exact in TF32; lo = x - hi); BF16 rounds to nearest
+//   warps 6-9  GEMM epilogue: TMEM lane quarter (warp % 4) -> Y rows, from a
+//              ring of AS accumulators, so the MMAs of later tiles overlap
+// Barriers (every wait bounded; one that runs out sets *err, and before the
+// CTA exits the producer waits, bounded, for its copies in flight and the
+// MMA lane for its MMAs):
+//   full[i]    copy bytes landed          rfree[i]  converters read the rows
+//   opr[i]     operands written           opf[i]    the MMAs read them
+//   accf[i]    accumulator complete       acce[i]   epilogue drained it
+// Operand layouts, no swizzle, 16-byte units:
+//   GEMM, K-major: tile row r, K unit u at u * 2048 + r * 16 (LBO 2048 B
+//     between K units, SBO 128 B between 8-row groups); B^T likewise.
+//   Gram, K = the tile's rows, M = 64 (D row m in TMEM lane (m % 16) +
+//     32 (m / 16)); A rows at or above M feed D rows that are never read.
+//     BF16: MN-major as the rows arrive, unit along M/N at unit * 2048 +
+//     row * 16 (SBO 2048, LBO 128); A's 8 units run past the real ones
+//     into memory the allocation covers.  3xTF32: K-major, element (m, k)
+//     at (k / 4) * LB + m * 16 + (k % 4) * 4 (LBO LB, SBO 128) with LB = 16
+//     bytes more than the real rows (128 * ceil(M / 8) for A, 16 Np for B),
+//     so the threads' 4-byte stores hit 32 banks; A's 64 rows per K unit
+//     overlap the next unit's rows, which only feeds unread D rows.
+// ---------------------------------------------------------------------------
+constexpr int kPipeRing = 8;
+constexpr int kGemmThreads = 320;
+constexpr size_t kPipeSmemBudget = size_t(200) << 10;   // the rings' target size
+constexpr size_t kPipeSmemMax = size_t(220) << 10;      // at most (227 KB per CTA, less the static part)
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+	asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+	asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// Bulk copy of `bytes` (a multiple of 16; both addresses 16-byte aligned)
+// from global to shared memory, completing on `bar` (no multicast).
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+	asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+			:: "r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+constexpr uint32_t instr_desc_m64(uint32_t fmt, uint32_t a_mn, uint32_t b_mn, uint32_t n)
+{
+	return (1u << 4) | (fmt << 7) | (fmt << 10) | (a_mn << 15) | (b_mn << 16) | ((n >> 3) << 17) | ((64u >> 4) << 24);
+}
+
+// Shared-memory plan of the pipelined kernels (host and device agree).
+struct pipe_plan {
+	bool gram, tf32;
+	int K, N, Kp, Np;                 // GEMM: X is n x K; Gram: X n x K (= M), W n x N
+	int64_t ldx, ldw;
+	size_t raw, op, acc_cols;         // bytes of a raw stage and an operand stage
+	size_t bpart;                     // GEMM: bytes of one part of B^T
+	size_t tail;                      // bytes the last operand stage's MMA reads past its end
+	int lba, lbb;                     // Gram 3xTF32: K-unit strides of A and B
+	size_t a_op, b_op;                // Gram: bytes of A and B operands (one part)
+	int RS, OS, AS;
+	size_t smem;
+	__host__ __device__ pipe_plan(bool gram_, bool tf32_, int K_, int N_, int64_t ldx_, int64_t ldw_)
+		: gram(gram_), tf32(tf32_), K(K_), N(N_), ldx(ldx_), ldw(ldw_)
+	{
+		const int KSTEP = tf32 ? 8 : 16;
+		Kp = (K + KSTEP - 1) / KSTEP * KSTEP;
+		Np = (N + 15) / 16 * 16;
+		raw = size_t(kTile) * 4 * size_t(ldx + (gram ? ldw : 0));
+		bpart = 0; tail = 0; lba = lbb = 0; a_op = b_op = 0;
+		if (!gram) {
+			const size_t part = tf32 ? size_t(Kp / 4) * kTile * 16 : size_t(Kp / 8) * kTile * 16;
+			op = (tf32 ? 2 : 1) * part;
+			bpart = tf32 ? size_t(Kp / 4) * Np * 16 : size_t(Kp / 8) * Np * 16;
+		} else if (tf32) {
+			lba = (K + 7) / 8 * 128 + 16;
+			lbb = Np * 16 + 16;
+			a_op = size_t(kTile / 4) * lba;
+			b_op = size_t(kTile / 4) * lbb;
+			op = 2 * (a_op + b_op);
+			// A's last K unit is read for 64 rows
+			tail = size_t(64 * 16) > size_t(lba) ? size_t(64 * 16 - lba) : 0;
+		} else {
+			a_op = size_t((K + 7) / 8) * kTile * 16;
+			b_op = size_t(Np / 8) * kTile * 16;
+			op = a_op + b_op;
+			tail = size_t(8) * kTile * 16 > a_op ? size_t(8) * kTile * 16 - a_op : 0;
+		}
+		AS = gram ? 1 : (Np <= 32 ? 8 : (Np <= 64 ? 4 : 2));
+		acc_cols = gram ? (Np <= 32 ? 32 : 64) : size_t(AS) * Np;
+		if (acc_cols < 32) acc_cols = 32;
+		// operand stages: 4 when they are small, else 2 (the raw stages carry
+		// the loads in flight); raw stages: as many as fit, up to the ring size
+		const size_t fixed = 2 * bpart + tail;
+		OS = (op <= 16384 && fixed + 4 * op + 6 * raw <= kPipeSmemBudget) ? 4 : 2;
+		RS = 2;
+		const size_t left = kPipeSmemBudget > fixed + size_t(OS) * op ? kPipeSmemBudget - fixed - size_t(OS) * op : 0;
+		RS = int(left / raw);
+		if (RS > kPipeRing) RS = kPipeRing;
+		if (RS < 2) RS = 2;
+		smem = size_t(RS) * raw + size_t(OS) * op + 2 * bpart + tail;
+	}
+	__host__ __device__ bool fits() const { return smem <= kPipeSmemMax; }
+};
+
+template <bool TF32, bool GRAM>
+__global__ void __launch_bounds__(kGemmThreads, 1)
+tc_pipe_kernel(const float *__restrict__ X, int64_t ldx, int K, const float *__restrict__ Wm, int64_t ldw, int N,
+		const float *__restrict__ B, int ldb, float *__restrict__ Y, int64_t ldy, float *__restrict__ part, int64_t n,
+		int *err)
+{
+	const pipe_plan P(GRAM, TF32, K, N, ldx, ldw);
+	constexpr int KSTEP = TF32 ? 8 : 16;
+	const int Kp = P.Kp, Np = P.Np, RS = P.RS, OS = P.OS, AS = P.AS;
+	extern __shared__ __align__(1024) char smem[];
+	// layout: raw ring, operand ring (plus the tail the last one reads), B^T
+	char *raw0 = smem;
+	char *op0 = smem + size_t(RS) * P.raw;
+	char *sb = op0 + size_t(OS) * P.op + P.tail;
+	__shared__ uint64_t full[kPipeRing], rfree[kPipeRing], opr[4], opf[4], accf[8], acce[8];
+	__shared__ uint32_t tmem_base;
+	__shared__ int bad;
+	const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+	const uint32_t ncols = P.acc_cols <= 32 ? 32 : (P.acc_cols <= 64 ? 64 : (P.acc_cols <= 128 ? 128 : 256));
+
+	for (size_t i = tid; i < P.smem / 16; i += blockDim.x) reinterpret_cast<uint4 *>(smem)[i] = make_uint4(0, 0, 0, 0);
+	__syncthreads();
+	if constexpr (!GRAM) {
+		for (int j = tid; j < Np; j += blockDim.x) {
+			float col[64];
+			for (int k = 0; k < Kp; k++) col[k] = (j < N && k < K) ? B[size_t(k) * ldb + j] : 0.f;
+			for (int pt = 0; pt < (TF32 ? 2 : 1); pt++) put_units<TF32>(sb + pt * P.bpart, Np * 16, j, col, Kp, Kp, pt);
+		}
+	}
+	if (warp == 1) tmem_alloc(&tmem_base, ncols);
+	if (tid == 0) {
+		for (int i = 0; i < RS; i++) { mbar_init(&full[i], 1); mbar_init(&rfree[i], 4); }
+		for (int i = 0; i < OS; i++) { mbar_init(&opr[i], 4); mbar_init(&opf[i], 1); }
+		for (int i = 0; i < AS; i++) { mbar_init(&accf[i], 1); mbar_init(&acce[i], 4); }
+		bad = 0;
+		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+	}
+	fence_async_smem();
+	tc_fence_before();
+	__syncthreads();
+	tc_fence_after();
+	const uint32_t tmem = tmem_base;
+	const int64_t ntiles = (n + kTile - 1) / kTile;
+	const int64_t my_tiles = int64_t(blockIdx.x) < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+	bool ok = true;
+	auto tile_row = [&](int64_t i) { return (int64_t(blockIdx.x) + i * int64_t(gridDim.x)) * kTile; };
+	// operand stage o: GEMM: part 1 (hi / BF16), part 2 (lo); Gram: A1 [A2] B1 [B2]
+	auto OPA1 = [&](int o) { return op0 + size_t(o) * P.op; };
+	auto OPA2 = [&](int o) { return OPA1(o) + (GRAM ? P.a_op : P.op / 2); };
+	auto OPB1 = [&](int o) { return OPA1(o) + (TF32 ? 2 : 1) * P.a_op; };
+	auto OPB2 = [&](int o) { return OPB1(o) + P.b_op; };
+
+	if (warp == 0) {
+		// ---- producer ----
+		if (lane == 0) {
+			int64_t issued = 0;
+			for (int64_t i = 0; i < my_tiles && ok; i++) {
+				const int s = int(i % RS);
+				if (i >= RS && !mbar_wait(&rfree[s], uint32_t((i / RS - 1) & 1))) { ok = false; break; }
+				const int64_t r0 = tile_row(i);
+				const int64_t rows = std::min<int64_t>(kTile, n - r0);
+				const uint32_t bx = uint32_t(rows * ldx * 4), bw = GRAM ? uint32_t(rows * ldw * 4) : 0u;
+				char *dst = raw0 + size_t(s) * P.raw;
+				mbar_expect_tx(&full[s], bx + bw);
+				bulk_load(dst, X + r0 * ldx, bx, &full[s]);
+				if (GRAM) bulk_load(dst + size_t(kTile) * 4 * size_t(ldx), Wm + r0 * ldw, bw, &full[s]);
+				issued = i + 1;
+			}
+			// copies still in flight must land before the CTA may exit
+			for (int64_t j = std::max<int64_t>(0, issued - RS); j < issued; j++)
+				if (!mbar_wait(&full[j % RS], uint32_t((j / RS) & 1))) ok = false;
+		}
+	} else if (warp == 1) {
+		// ---- MMA issuer ----
+		if (lane == 0) {
+			uint32_t idesc;
+			if constexpr (GRAM) idesc = TF32 ? instr_desc_m64(2, 0, 0, uint32_t(Np)) : instr_desc_m64(1, 1, 1, uint32_t(Np));
+			else idesc = instr_desc(TF32 ? 2 : 1, 0, 0, uint32_t(Np));
+			// descriptors once: the start address is the low field (16-byte
+			// units), so an operand at byte offset `off` from the base is the
+			// base descriptor plus off / 16 (shared addresses stay < 256 KB)
+			uint64_t dA, dB;
+			uint32_t a_step, b_step, a_pass2 = 0, b_pass1 = 0;
+			if constexpr (!GRAM) {
+				dA = smem_desc(smem_u32(op0), kTile * 16, 128);
+				dB = smem_desc(smem_u32(sb), Np * 16, 128);
+				a_step = 2 * kTile * 16 / 16;
+				b_step = 2 * Np * 16 / 16;
+				a_pass2 = uint32_t(P.op / 2 / 16);
+				b_pass1 = uint32_t(P.bpart / 16);
+			} else if constexpr (TF32) {
+				dA = smem_desc(smem_u32(op0), P.lba, 128);
+				dB = smem_desc(smem_u32(op0) + uint32_t(2 * P.a_op), P.lbb, 128);
+				a_step = 2 * P.lba / 16;
+				b_step = 2 * P.lbb / 16;
+				a_pass2 = uint32_t(P.a_op / 16);
+				b_pass1 = uint32_t(P.b_op / 16);
+			} else {
+				dA = smem_desc(smem_u32(op0), 128, kTile * 16);
+				dB = smem_desc(smem_u32(op0) + uint32_t(P.a_op), 128, kTile * 16);
+				a_step = b_step = 2 * 128 / 16;
+			}
+			const int nks = GRAM ? kTile / KSTEP : Kp / KSTEP;
+			int64_t issued = 0;
+			uint32_t acc = 0;
+			for (int64_t i = 0; i < my_tiles && ok; i++) {
+				const int o = int(i % OS), b = int(i % AS);
+				if (!GRAM && i >= AS && !mbar_wait(&acce[b], uint32_t((i / AS - 1) & 1))) { ok = false; break; }
+				if (!mbar_wait(&opr[o], uint32_t((i / OS) & 1))) { ok = false; break; }
+				tc_fence_after();
+				const uint64_t stage_off = uint64_t(o) * (P.op / 16);
+				const uint32_t d = GRAM ? tmem : tmem + uint32_t(b * Np);
+				if constexpr (!GRAM) acc = 0;
+				for (int pass = 0; pass < (TF32 ? 3 : 1); pass++) {
+					// (hi, hi), (hi, lo), (lo, hi)
+					uint64_t a = dA + stage_off + (pass == 2 ? a_pass2 : 0);
+					uint64_t bd = dB + (GRAM ? stage_off : 0) + (pass == 1 ? b_pass1 : 0);
+					for (int ks = 0; ks < nks; ks++) {
+						umma<TF32>(d, a, bd, idesc, acc);
+						acc = 1;
+						a += a_step;
+						bd += b_step;
+					}
+				}
+				umma_commit(&opf[o]);
+				if constexpr (!GRAM) umma_commit(&accf[b]);
+				issued = i + 1;
+			}
+			if constexpr (GRAM) {
+				umma_commit(&accf[0]);
+			} else {
+				// the MMAs issued must be complete before TMEM is released
+				if (issued && !mbar_wait(&accf[(issued - 1) % AS], uint32_t(((issued - 1) / AS) & 1))) ok = false;
+			}
+		}
+	} else if (warp < 6) {
+		// ---- converters ----
+		const int r = tid - 64;
+		for (int64_t i = 0; i < my_tiles && ok; i++) {
+			const int s = int(i % RS), o = int(i % OS);
+			if (!mbar_wait(&full[s], uint32_t((i / RS) & 1))) { ok = false; break; }
+			if (i >= OS && !mbar_wait(&opf[o], uint32_t((i / OS - 1) & 1))) { ok = false; break; }
+			const bool live = tile_row(i) + r < n;
+			const char *rs = raw0 + size_t(s) * P.raw;
+			for (int side = 0; side < (GRAM ? 2 : 1); side++) {
+				const int L = side ? N : K;
+				const int64_t ld = side ? ldw : ldx;
+				const float *xr = reinterpret_cast<const float *>(rs + (side ? size_t(kTile) * 4 * size_t(ldx) : 0) +
+						size_t(r) * size_t(ld) * 4);
+				if (TF32 && GRAM) {
+					// K-major transpose (4-byte stores, 32 banks per warp)
+					char *o1 = side ? OPB1(o) : OPA1(o), *o2 = side ? OPB2(o) : OPA2(o);
+					const int lb = side ? P.lbb : P.lba;
+					char *b1 = o1 + size_t(r / 4) * lb + (r % 4) * 4, *b2 = o2 + size_t(r / 4) * lb + (r % 4) * 4;
+					const int units = (L + 3) / 4;
+					int u = r % units;                   // rotated start: the reads of a wavefront spread over banks
+					for (int u0 = 0; u0 < units; u0++, u = (u + 1 == units) ? 0 : u + 1) {
+						float xs[4];
+#pragma unroll
+						for (int q = 0; q < 4; q++) xs[q] = 0.f;
+						if (live) {
+							if (4 * u + 3 < L) {
+								const float4 x = reinterpret_cast<const float4 *>(xr)[u];
+								xs[0] = x.x; xs[1] = x.y; xs[2] = x.z; xs[3] = x.w;
+							} else {
+								for (int q = 0; 4 * u + q < L; q++) xs[q] = xr[4 * u + q];
+							}
+						}
+#pragma unroll
+						for (int q = 0; q < 4; q++) {
+							const int m = 4 * u + q;
+							if (m < L) {
+								const uint32_t hb = __float_as_uint(xs[q]) & 0xFFFFE000u;
+								*reinterpret_cast<uint32_t *>(b1 + size_t(m) * 16) = hb;
+								*reinterpret_cast<float *>(b2 + size_t(m) * 16) = __fsub_rn(xs[q], __uint_as_float(hb));
+							}
+						}
+					}
+				} else if (TF32) {
+					// GEMM, K-major units of 4: hi and lo; the row's loads go first
+					char *o1 = OPA1(o), *o2 = OPA2(o);
+					const int units = K / 4;
+					float4 xv[16];
+					const int rot = r % units;           // rotated start: a wavefront's reads spread over banks
+#pragma unroll
+					for (int u0 = 0; u0 < 16; u0++)
+						if (u0 < units) {
+							const int u = u0 + rot < units ? u0 + rot : u0 + rot - units;
+							xv[u0] = live ? reinterpret_cast<const float4 *>(xr)[u] : make_float4(0.f, 0.f, 0.f, 0.f);
+						}
+#pragma unroll
+					for (int u0 = 0; u0 < 16; u0++)
+						if (u0 < units) {
+							const int u = u0 + rot < units ? u0 + rot : u0 + rot - units;
+							const uint32_t xs[4] = {__float_as_uint(xv[u0].x), __float_as_uint(xv[u0].y),
+									__float_as_uint(xv[u0].z), __float_as_uint(xv[u0].w)};
+							uint32_t hi[4], lo[4];
+#pragma unroll
+							for (int q = 0; q < 4; q++) {
+								hi[q] = xs[q] & 0xFFFFE000u;
+								lo[q] = __float_as_uint(__fsub_rn(__uint_as_float(xs[q]), __uint_as_float(hi[q])));
+							}
+							*reinterpret_cast<uint4 *>(o1 + size_t(u) * kTile * 16 + size_t(r) * 16) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+							*reinterpret_cast<uint4 *>(o2 + size_t(u) * kTile * 16 + size_t(r) * 16) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+						}
+				} else {
+					// BF16 units of 8 (GEMM K-major, Gram MN-major: the same writes)
+					char *o1 = GRAM ? (side ? OPB1(o) : OPA1(o)) : OPA1(o);
+					const int units = (L + 7) / 8;
+					int u = r % units;
+					for (int u0 = 0; u0 < units; u0++, u = (u + 1 == units) ? 0 : u + 1) {
+						float xs[8];
+						if (live && 8 * u + 8 <= L) {
+							const float4 a4 = reinterpret_cast<const float4 *>(xr)[2 * u];
+							const float4 c4 = reinterpret_cast<const float4 *>(xr)[2 * u + 1];
+							xs[0] = a4.x; xs[1] = a4.y; xs[2] = a4.z; xs[3] = a4.w;
+							xs[4] = c4.x; xs[5] = c4.y; xs[6] = c4.z; xs[7] = c4.w;
+						} else {
+#pragma unroll
+							for (int q = 0; q < 8; q++) xs[q] = (live && 8 * u + q < L) ? xr[8 * u + q] : 0.f;
+						}
+						uint32_t w[4];
+#pragma unroll
+						for (int q = 0; q < 4; q++) {
+							__nv_bfloat162 h = __floats2bfloat162_rn(xs[2 * q], xs[2 * q + 1]);
+							memcpy(&w[q], &h, 4);
+						}
+						*reinterpret_cast<uint4 *>(o1 + size_t(u) * kTile * 16 + size_t(r) * 16) = make_uint4(w[0], w[1], w[2], w[3]);
+					}
+				}
+			}
+			fence_async_smem();
+			__syncwarp();
+			if (lane == 0) { mbar_arrive(&rfree[s]); mbar_arrive(&opr[o]); }
+		}
+		if constexpr (GRAM) {
+			// read out D: warp quarter q holds rows 16 q .. 16 q + 15 in lanes 32 q .. 32 q + 15
+			const bool done = ok && mbar_wait(&accf[0], 0);
+			const bool all = __all_sync(0xffffffffu, done);
+			ok = ok && done;
+			if (all) {
+				tc_fence_after();
+				const int q = warp & 3;
+				const int m = 16 * q + lane;
+				for (int c0 = 0; c0 < Np; c0 += 16) {
+					float o[16];
+					tmem_ld16(tmem + (uint32_t(q * 32) << 16) + uint32_t(c0), o);
+					if (lane < 16 && m < K)
+						for (int c = 0; c < 16 && c0 + c < N; c++)
+							part[(size_t(blockIdx.x) * K + m) * N + c0 + c] = my_tiles ? o[c] : 0.f;
+				}
+			}
+		}
+	} else if constexpr (!GRAM) {
+		// ---- GEMM epilogue: TMEM lanes 32q..32q+31 = tile rows ----
+		const int q = warp & 3;
+		const bool vy = (N % 4) == 0 && (ldy % 4) == 0 && (reinterpret_cast<uintptr_t>(Y) & 15) == 0;
+		for (int64_t i = 0; i < my_tiles && ok; i++) {
+			const int b = int(i % AS);
+			if (!mbar_wait(&accf[b], uint32_t((i / AS) & 1))) { ok = false; break; }
+			tc_fence_after();
+			const int64_t row = tile_row(i) + q * 32 + lane;
+			for (int c0 = 0; c0 < Np; c0 += 16) {
+				float o[16];
+				tmem_ld16(tmem + (uint32_t(q * 32) << 16) + uint32_t(b * Np + c0), o);
+				if (row < n) {
+					if (vy && c0 + 16 <= N) {
+						float4 *yr = reinterpret_cast<float4 *>(Y + row * ldy + c0);
+#pragma unroll
+						for (int v = 0; v < 4; v++) yr[v] = make_float4(o[4 * v], o[4 * v + 1], o[4 * v + 2], o[4 * v + 3]);
+					} else {
+						for (int c = 0; c < 16 && c0 + c < N; c++) Y[row * ldy + c0 + c] = o[c];
+					}
+				}
+			}
+			tc_fence_before();
+			__syncwarp();
+			if (lane == 0) mbar_arrive(&acce[b]);
+		}
+	}
+	if (!ok) atomicExch(&bad, 1);
+	tc_fence_before();
+	__syncthreads();
+	tc_fence_after();
+	if (tid == 0 && bad) atomicExch(err, 1);
+	if (warp == 1) tmem_dealloc(tmem, ncols);
+}
+
+// ---------------------------------------------------------------------------
 // G (M x N) = X^T W over row chunks of 128: A = X^T chunk and B = W chunk are
 // MN-major (rows of X and W are contiguous along M and N).  Core matrix =
 // 8 chunk rows x 16 bytes; LBO = 128 B between 8-row groups, SBO = 16 groups
@@ -789,10 +1190,24 @@ int fmx_dense_gemm(int precision, const float *X, int64_t ldx, int64_t n, int K,
 	const bool tf32 = precision == FMX_DENSE_TF32X3;
 	const int E = tf32 ? 4 : 8, KSTEP = tf32 ? 8 : 16, parts = tf32 ? 2 : 1;
 	const int Kp = (K + KSTEP - 1) / KSTEP * KSTEP, Np = (N + 15) / 16 * 16;
-	const size_t smem = size_t(parts) * (size_t(Kp / E) * kTile * 16 + size_t(Kp / E) * Np * 16);
 	int dev = 0;
 	cudaGetDevice(&dev);
 	const int64_t tiles = (n + kTile - 1) / kTile;
+	cudaStream_t st = static_cast<cudaStream_t>(stream);
+	// the pipelined kernel when the rows of X can be bulk-copied (16-byte
+	// aligned rows of whole 16-byte units)
+	if (K % 4 == 0 && ldx % 4 == 0 && ldx <= 64 && (reinterpret_cast<uintptr_t>(X) & 15) == 0 && n > 0) {
+		const pipe_plan P(false, tf32, K, N, ldx, 0);
+		if (P.fits()) {
+			auto kern = tf32 ? tc_pipe_kernel<true, false> : tc_pipe_kernel<false, false>;
+			DCUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(P.smem)));
+			const unsigned grid = unsigned(std::max<int64_t>(1, std::min<int64_t>(tiles, int64_t(sms(dev)))));
+			kern<<<grid, kGemmThreads, P.smem, st>>>(X, ldx, K, nullptr, 0, N, B, ldb, Y, ldy, nullptr, n, err);
+			DCUDA_TRY(cudaGetLastError());
+			return FMX_OK;
+		}
+	}
+	const size_t smem = size_t(parts) * (size_t(Kp / E) * kTile * 16 + size_t(Kp / E) * Np * 16);
 	// as many CTAs per SM as registers and shared memory allow, but no more
 	// than the SM's 512 TMEM columns hold (each CTA allocates tmem_cols)
 	const int tmem_cols = Np <= 32 ? 32 : (Np <= 64 ? 64 : 128);
@@ -802,7 +1217,6 @@ int fmx_dense_gemm(int precision, const float *X, int64_t ldx, int64_t n, int K,
 	DCUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, smem));
 	per_sm = std::max(1, std::min(per_sm, 512 / tmem_cols));
 	const unsigned grid = unsigned(std::max<int64_t>(1, std::min<int64_t>(tiles, int64_t(sms(dev)) * per_sm)));
-	cudaStream_t st = static_cast<cudaStream_t>(stream);
 	kern<<<grid, 128, smem, st>>>(X, ldx, K, B, ldb, N, Y, ldy, n, err);
 	DCUDA_TRY(cudaGetLastError());
 	return FMX_OK;
@@ -815,6 +1229,8 @@ int fmx_dense_gram_parts(int precision, int64_t n)
 	const int64_t chunks = (n + kTile - 1) / kTile;
 	if (precision == FMX_DENSE_F64) return int(std::max<int64_t>(1, std::min<int64_t>((n + 63) / 64, int64_t(sms(dev)) * 4)));
 	return int(std::max<int64_t>(1, std::min<int64_t>(chunks, int64_t(sms(dev)) * (precision == FMX_DENSE_TF32X3 ? 1 : 2))));
+	// (the pipelined tensor-core Gram runs one CTA per SM, the older kernel up
+	// to two: callers size their partials with this count either way)
 }
 
 int fmx_dense_gram(int precision, const float *X, int64_t ldx, int M, const float *W, int64_t ldw, int N, int64_t n,
@@ -838,6 +1254,22 @@ int fmx_dense_gram(int precision, const float *X, int64_t ldx, int M, const floa
 	if (!err) return set_error(FMX_ERR_INVAL, "null error flag");
 	const bool tf32 = precision == FMX_DENSE_TF32X3;
 	if (!tf32 && precision != FMX_DENSE_BF16) return set_error(FMX_ERR_INVAL, "unknown precision %d", precision);
+	if (ldx % 4 == 0 && ldw % 4 == 0 && ldx <= 64 && ldw <= 64 && (reinterpret_cast<uintptr_t>(X) & 15) == 0 &&
+			(reinterpret_cast<uintptr_t>(W) & 15) == 0 && n > 0) {
+		const pipe_plan P(true, tf32, M, N, ldx, ldw);
+		if (P.fits()) {
+			// the pipelined kernel: one CTA per SM, partials reduced in CTA order
+			auto kern = tf32 ? tc_pipe_kernel<true, true> : tc_pipe_kernel<false, true>;
+			DCUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(P.smem)));
+			kern<<<parts, kGemmThreads, P.smem, st>>>(X, ldx, M, W, ldw, N, nullptr, 0, nullptr, 0,
+					static_cast<float *>(part), n, err);
+			DCUDA_TRY(cudaGetLastError());
+			gram_reduce_kernel<float><<<(M * N + 7) / 8, 256, 0, st>>>(static_cast<const float *>(part), parts, M * N,
+					static_cast<float *>(G));
+			DCUDA_TRY(cudaGetLastError());
+			return FMX_OK;
+		}
+	}
 	const int Np = (N + 15) / 16 * 16;
 	const size_t smem = tf32 ? size_t(2) * (size_t(kTile / 4) * kTile * 16 + size_t(kTile / 4) * Np * 16)
 	                         : size_t(kTile / 8) * 2048 + size_t(Np / 8) * 2048;

@@ -446,6 +446,11 @@ __device__ __forceinline__ void store_row(const spmm_args &a, int32_t row, int c
 template <int U>
 __device__ __forceinline__ void ld_idx(const uint32_t *col, uint32_t step, uint32_t (&r)[U])
 {
+	if constexpr (U == 2) {
+		const uint2 a = __ldg(reinterpret_cast<const uint2 *>(col) + step);
+		r[0] = a.x; r[1] = a.y;
+		return;
+	}
 	const uint4 *p = reinterpret_cast<const uint4 *>(col) + (U / 4) * step;
 #pragma unroll
 	for (int q = 0; q < U / 4; q++) {
@@ -462,15 +467,25 @@ __device__ __forceinline__ void ld_w(const void *val, uint32_t step, A (&w)[U])
 #pragma unroll
 		for (int u = 0; u < U; u++) w[u] = A(1);
 	} else {
-		const uint4 *p = reinterpret_cast<const uint4 *>(static_cast<const WT *>(val) + size_t(step) * U);
-		constexpr int per = int(16 / sizeof(WT));
+		if constexpr (U * sizeof(WT) == 8) {
+			// two 4-byte weights (a step of 2 entries)
+			const uint2 b = __ldcs(reinterpret_cast<const uint2 *>(static_cast<const WT *>(val) + size_t(step) * U));
+			WT t[2];
+			memcpy(t, &b, 8);
+			w[0] = A(t[0]);
+			w[1] = A(t[1]);
+		} else {
+			const uint4 *p = reinterpret_cast<const uint4 *>(static_cast<const WT *>(val) + size_t(step) * U);
+			constexpr int per = int(16 / sizeof(WT));
+			static_assert(U % per == 0, "whole 16-byte weight loads");
 #pragma unroll
-		for (int q = 0; q < U / per; q++) {
-			uint4 a = __ldcs(p + q);
-			WT t[per];
-			memcpy(t, &a, 16);
+			for (int q = 0; q < U / per; q++) {
+				uint4 a = __ldcs(p + q);
+				WT t[per];
+				memcpy(t, &a, 16);
 #pragma unroll
-			for (int i = 0; i < per; i++) w[q * per + i] = A(t[i]);
+				for (int i = 0; i < per; i++) w[q * per + i] = A(t[i]);
+			}
 		}
 	}
 }
@@ -612,6 +627,159 @@ spmm_kernel(const spmm_args a, const pr_epi e)
 		cnt = __reduce_add_sync(0xffffffffu, cnt);
 		if (lane == 0 && cnt) atomicAdd(e.state, (unsigned long long)cnt);
 	}
+}
+
+// ---------------------------------------------------------------------------
+// 32-byte lanes (the main path for row panels of 32, 64 or 128 bytes).
+//
+// A lane owns 32 bytes of every X row it gathers (8 FP32 or 16 BF16
+// elements), so a row panel of P bytes takes G = P / 32 lanes (1, 2 or 4) and
+// a warp runs 32 / G lane groups.  Each entry costs one 256-bit load per lane
+// and one decode per lane (the 16-byte-lane kernel spends a decode on every
+// 16 bytes); a warp-wide load still touches one 128-byte line per row.
+// Loads use no L2 policy: the measured gain of the hot/cold hints did not pay
+// for selecting them per entry.  The arithmetic is the 16-byte-lane kernel's
+// (products rounded, adds in entry order as packed FP32 pairs), so results
+// are bit-identical.
+// ---------------------------------------------------------------------------
+#ifndef FMX_WIDE_MIN_BLOCKS
+#define FMX_WIDE_MIN_BLOCKS 4
+#endif
+#ifndef FMX_WIDE_STEP
+#define FMX_WIDE_STEP 4
+#endif
+
+__device__ __forceinline__ void ld32_nc(const void *p, uint32_t (&r)[8])
+{
+	asm volatile("ld.global.nc.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+			: "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+			: "l"(p));
+}
+// 32-byte streaming store when `pred` holds (predicated, no branch).
+__device__ __forceinline__ void st32_if(void *p, const uint32_t (&v)[8], bool pred)
+{
+	asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %9, 0;\n\t"
+			"@q st.global.cs.v8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};\n\t}"
+			:: "l"(p), "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]),
+			   "r"(uint32_t(pred)) : "memory");
+}
+
+// The VEC elements of one 32-byte load as FP32 (BF16 widened exactly).
+template <class XT, int VEC>
+__device__ __forceinline__ void widen(const uint32_t (&r)[8], float (&f)[VEC])
+{
+	if constexpr (sizeof(XT) == 4) {
+#pragma unroll
+		for (int i = 0; i < 8; i++) f[i] = __uint_as_float(r[i]);
+	} else {
+#pragma unroll
+		for (int i = 0; i < 8; i++) {
+			f[2 * i] = __uint_as_float(r[i] << 16);
+			f[2 * i + 1] = __uint_as_float(r[i] & 0xFFFF0000u);
+		}
+	}
+}
+
+template <class XT, class YT, class WT, int U, bool SCALE_IN, bool SCALE_OUT>
+__device__ __forceinline__ void run_range_wide(const spmm_args &a, const range_t rg, int colbase)
+{
+	constexpr int VEC = int(32 / sizeof(XT));
+	constexpr bool kBinary = std::is_void<WT>::value;
+	const char *Xb = static_cast<const char *>(a.X) + size_t(colbase) * sizeof(XT);
+	const char *Hb = static_cast<const char *>(a.xhot) + size_t(colbase) * sizeof(XT);
+	const uint32_t xs = uint32_t(a.ldx) * uint32_t(sizeof(XT)), hs = uint32_t(a.hot_ld) * uint32_t(sizeof(XT));
+	char *Yb = static_cast<char *>(a.Y) + size_t(colbase) * sizeof(YT);
+	const uint64_t ys = uint64_t(a.ldy) * sizeof(YT);
+	const bool runs = rg.slot == kNoSlot;
+	uint64_t p[VEC / 2];
+#pragma unroll
+	for (int i = 0; i < VEC / 2; i++) p[i] = 0;
+	uint32_t row = rg.row0;
+	uint32_t s = rg.e0 / U;
+	const uint32_t s_end = s + rg.len / U;
+	uint32_t raw[U];
+	ld_idx<U>(a.col, s, raw);
+	for (; s < s_end; s++) {
+		float w[U];
+		if constexpr (!kBinary) ld_w<WT, float, U>(a.val, s, w);
+		uint32_t xv[U][8];
+		float sc[U];
+		uint32_t ends = 0;
+#pragma unroll
+		for (int u = 0; u < U; u++) {
+			const uint32_t c = raw[u] & kIdxMask;
+			const bool hot = raw[u] & kHot;
+			ld32_nc((hot ? Hb : Xb) + uint64_t(c) * (hot ? hs : xs), xv[u]);
+			if constexpr (SCALE_IN) sc[u] = hot ? 1.f : static_cast<const float *>(a.s_in)[c];
+			ends |= (raw[u] >> 31) << u;
+		}
+		if (s + 1 < s_end) ld_idx<U>(a.col, s + 1, raw);
+#pragma unroll
+		for (int u = 0; u < U; u++) {
+			float f[VEC];
+			widen<XT, VEC>(xv[u], f);
+#pragma unroll
+			for (int i = 0; i < VEC / 2; i++) {
+				float t0 = f[2 * i], t1 = f[2 * i + 1];
+				// (x * s_in) * w, each product rounded, like scale_rows then SpMM
+				if constexpr (SCALE_IN) { t0 = __fmul_rn(t0, sc[u]); t1 = __fmul_rn(t1, sc[u]); }
+				if constexpr (!kBinary) { t0 = __fmul_rn(t0, w[u]); t1 = __fmul_rn(t1, w[u]); }
+				p[i] = add2(p[i], pack2(t0, t1));
+			}
+			const bool end = runs && ((ends >> u) & 1u);
+			float so = 1.f;
+			if constexpr (SCALE_OUT) so = end ? static_cast<const float *>(a.s_out)[row] : 1.f;
+			float o[VEC];
+#pragma unroll
+			for (int i = 0; i < VEC / 2; i++) {
+				unpack2(p[i], o[2 * i], o[2 * i + 1]);
+				if constexpr (SCALE_OUT) { o[2 * i] = __fmul_rn(o[2 * i], so); o[2 * i + 1] = __fmul_rn(o[2 * i + 1], so); }
+			}
+			char *yp = Yb + uint64_t(row) * ys;
+			if constexpr (sizeof(YT) == 4) {
+#pragma unroll
+				for (int h = 0; h < VEC / 8; h++) {
+					uint32_t v[8];
+#pragma unroll
+					for (int i = 0; i < 8; i++) v[i] = __float_as_uint(o[8 * h + i]);
+					st32_if(yp + 32 * h, v, end);
+				}
+			} else {
+				uint32_t v[8];
+#pragma unroll
+				for (int i = 0; i < 8; i++) {
+					__nv_bfloat162 b2 = __floats2bfloat162_rn(o[2 * i], o[2 * i + 1]);
+					memcpy(&v[i], &b2, 4);
+				}
+				st32_if(yp, v, end);
+			}
+#pragma unroll
+			for (int i = 0; i < VEC / 2; i++) p[i] = end ? 0ull : p[i];
+			row += end;
+		}
+	}
+	if (!runs) {
+		float *q = static_cast<float *>(a.partial) + int64_t(rg.slot) * kPartialStride + colbase;
+#pragma unroll
+		for (int i = 0; i < VEC / 2; i++) unpack2(p[i], q[2 * i], q[2 * i + 1]);
+	}
+}
+
+template <class XT, class YT, class WT, int U, bool SCALE_IN, bool SCALE_OUT>
+__global__ void __launch_bounds__(kThreads, FMX_WIDE_MIN_BLOCKS) spmm_wide_kernel(const spmm_args a)
+{
+	constexpr int VEC = int(32 / sizeof(XT));
+	const int lane = threadIdx.x & 31;
+	const uint32_t gw = (blockIdx.x * kThreads + threadIdx.x) >> 5;
+	const uint32_t nw = (gridDim.x * kThreads) >> 5;
+	const int G = a.G, R = a.R;
+	const int grp = lane / G;
+	if (grp >= R) return;
+	const int colbase = (lane - grp * G) * VEC;
+	const uint32_t gg = gw * uint32_t(R) + uint32_t(grp);
+	const uint32_t ng = nw * uint32_t(R);
+	for (uint32_t r = gg; r < a.n_ranges; r += ng)
+		run_range_wide<XT, YT, WT, U, SCALE_IN, SCALE_OUT>(a, a.ranges[r], colbase);
 }
 
 // k = 1 (SpMV): a warp per range.  The 32 lanes load the range's column ids
@@ -1270,8 +1438,20 @@ static int launch_one(const gpu_part &p, const spmm_args &a, cudaStream_t st)
 	return FMX_OK;
 }
 
+template <class XT, class YT, class WT, bool SI, bool SO>
+static int launch_wide(const gpu_part &p, const spmm_args &a, cudaStream_t st)
+{
+	// BF16 lanes hold 16 elements: a step of 2 entries keeps them in registers
+	auto kern = spmm_wide_kernel<XT, YT, WT, sizeof(XT) == 2 ? 2 : FMX_WIDE_STEP, SI, SO>;
+	static std::atomic<unsigned> blocks[64];
+	const unsigned b = cached_blocks(blocks[p.device & 63], kern, p.device);
+	kern<<<b, kThreads, 0, st>>>(a);
+	CUDA_TRY(cudaGetLastError());
+	return FMX_OK;
+}
+
 template <class XT, class YT, class A, class WT, int VEC, int NV>
-static int launch_t(const gpu_part &p, spmm_args a, bool sin, bool sout, cudaStream_t st)
+static int launch_t(const gpu_part &p, spmm_args a, bool sin, bool sout, cudaStream_t st, bool wide = false)
 {
 	{
 		const uint64_t total = uint64_t(p.n_hot + 1) * a.k;
@@ -1283,6 +1463,14 @@ static int launch_t(const gpu_part &p, spmm_args a, bool sin, bool sout, cudaStr
 		CUDA_TRY(cudaGetLastError());
 	}
 	int rc = over_slices(p, a, st, [&](const spmm_args &sa) -> int {
+		if constexpr (std::is_same<A, float>::value && (std::is_same<WT, void>::value || std::is_same<WT, float>::value)) {
+			if (wide) {
+				if (sin && sout) return launch_wide<XT, YT, WT, true, true>(p, sa, st);
+				if (sin) return launch_wide<XT, YT, WT, true, false>(p, sa, st);
+				if (sout) return launch_wide<XT, YT, WT, false, true>(p, sa, st);
+				return launch_wide<XT, YT, WT, false, false>(p, sa, st);
+			}
+		}
 		if (sin && sout) return launch_one<XT, YT, A, WT, VEC, NV, true, true>(p, sa, st);
 		if (sin) return launch_one<XT, YT, A, WT, VEC, NV, true, false>(p, sa, st);
 		if (sout) return launch_one<XT, YT, A, WT, VEC, NV, false, true>(p, sa, st);
@@ -1298,23 +1486,27 @@ static int launch_t(const gpu_part &p, spmm_args a, bool sin, bool sout, cudaStr
 }
 
 static bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+static bool aligned32(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 31) == 0; }
 
 // Run one orientation over all column panels (kPanelBytes of X row each).
 // k = 1 without row scales: pack, the warp-per-range SpMV, fixup.
+// `xhot` and `partial` default to the part's own scratch.
 template <class T, class WT, bool EPI>
 static int run_spmv(const gpu_part &p, const T *X, int64_t ldx, T *Y, int64_t ldy, cudaStream_t st,
-		const pr_epi &e = pr_epi{})
+		const pr_epi &e = pr_epi{}, void *xhot = nullptr, void *partial = nullptr)
 {
+	if (!xhot) xhot = p.xhot;
+	if (!partial) partial = p.partial;
 	spmm_args a{};
 	a.col = p.col; a.val = p.val; a.ranges = p.ranges;
-	a.X = X; a.xhot = p.xhot; a.hot_ld = 1;
+	a.X = X; a.xhot = xhot; a.hot_ld = 1;
 	a.Y = Y;
-	a.partial = p.partial;
+	a.partial = partial;
 	a.ldx = ldx; a.ldy = ldy; a.k = 1;
 	a.G = 1; a.R = 32; a.nv = 1;
 	a.n_ranges = p.n_ranges;
 	const unsigned pb = unsigned(std::min<uint64_t>((uint64_t(p.n_hot) + 256) / 256, 148ull * 16));
-	pack_hot_kernel<T, T, false><<<pb, 256, 0, st>>>(p.hot_col, p.n_hot, X, ldx, 1, static_cast<T *>(p.xhot), 1,
+	pack_hot_kernel<T, T, false><<<pb, 256, 0, st>>>(p.hot_col, p.n_hot, X, ldx, 1, static_cast<T *>(xhot), 1,
 			nullptr);
 	CUDA_TRY(cudaGetLastError());
 	auto kern = spmv_kernel<T, WT, EPI>;
@@ -1326,7 +1518,7 @@ static int run_spmv(const gpu_part &p, const T *X, int64_t ldx, T *Y, int64_t ld
 			return FMX_OK;
 		}))
 		return rc;
-	return launch_fixup<T, T, false, EPI>(p, static_cast<const T *>(p.partial), Y, ldy, 1, nullptr, st, e);
+	return launch_fixup<T, T, false, EPI>(p, static_cast<const T *>(partial), Y, ldy, 1, nullptr, st, e);
 }
 
 template <class XT, class YT, class A, class WT>
@@ -1355,7 +1547,16 @@ static int run_typed(const gpu_part &p, const void *X, int64_t ldx, void *Y, int
 		a.ldx = ldx; a.ldy = ldy; a.k = kp;
 		a.n_ranges = p.n_ranges;
 		int rc;
-		if (vec_ok) {
+		// 32-byte lanes: FP32 accumulation, a panel of whole 32-byte lanes,
+		// X, Y and the packed rows 32-byte aligned
+		const bool wide = std::is_same<A, float>::value && vec_ok && (kp * sizeof(XT)) % 32 == 0 &&
+				(ldx * sizeof(XT)) % 32 == 0 && (ldy * sizeof(YT)) % 32 == 0 && aligned32(a.X) && aligned32(a.Y);
+		if (wide) {
+			a.G = int(kp * sizeof(XT) / 32);     // 1, 2 or 4
+			a.R = 32 / a.G;
+			a.nv = 1;
+			rc = launch_t<XT, YT, A, WT, VEC, 1>(p, a, sin, sout, st, true);
+		} else if (vec_ok) {
 			a.G = kp / VEC;           // <= 8
 			a.R = 32 / a.G;
 			a.nv = 1;
@@ -1910,6 +2111,8 @@ template <class WT>
 static int run_noalloc(const gpu_part &p, const float *X, int64_t ldx, float *Y, int64_t ldy, int64_t k,
 		void *xhot, void *partial, cudaStream_t st)
 {
+	// the kernels fmx_spmm runs for the same call, on the fixed scratch
+	if (k == 1) return run_spmv<float, WT, false>(p, X, ldx, Y, ldy, st, pr_epi{}, xhot, partial);
 	constexpr int VEC = 4;
 	constexpr int kPanel = kPanelBytes / int(sizeof(float));
 	const bool vec_ok = (k % VEC == 0) && (ldx % VEC == 0) && (ldy % VEC == 0) && aligned16(X) && aligned16(Y);

@@ -22,16 +22,21 @@ def _stream(torch):
 
 
 @pytest.mark.parametrize("prec", [_lib.DENSE_BF16, _lib.DENSE_TF32X3])
-@pytest.mark.parametrize("n,K,N", [(1000, 16, 16), (100003, 16, 16), (50000, 32, 16), (7777, 48, 32), (300, 8, 64),
-                                   (130, 64, 48)])
-def test_tc_gemm(torch_cuda, prec, n, K, N):
+@pytest.mark.parametrize("n,K,N,ldx", [(1000, 16, 16, 16), (100003, 16, 16, 16), (50000, 32, 16, 32),
+                                       (7777, 48, 32, 48), (300, 8, 64, 8), (130, 64, 48, 64),
+                                       # K padded to the MMA step; rows wider than K
+                                       (999, 12, 24, 12), (4097, 20, 16, 24), (70000, 16, 16, 20),
+                                       # K % 4 != 0: the thread-staged kernel
+                                       (5000, 10, 16, 10), (333, 3, 8, 7)])
+def test_tc_gemm(torch_cuda, prec, n, K, N, ldx):
     torch = torch_cuda
     g = torch.Generator(device="cuda").manual_seed(n + K)
-    X = torch.randn((n, K), generator=g, device="cuda")
+    Xf = torch.randn((n, ldx), generator=g, device="cuda")
+    X = Xf[:, :K]
     B = torch.randn((K, N), generator=g, device="cuda")
     Y = torch.full((n, N), float("nan"), device="cuda")
     err = torch.zeros(1, dtype=torch.int32, device="cuda")
-    rc = _lib.lib.fmx_dense_gemm(prec, X.data_ptr(), K, n, K, B.data_ptr(), N, N, Y.data_ptr(), N, err.data_ptr(),
+    rc = _lib.lib.fmx_dense_gemm(prec, Xf.data_ptr(), ldx, n, K, B.data_ptr(), N, N, Y.data_ptr(), N, err.data_ptr(),
                                  _stream(torch))
     assert rc == 0, _lib.last_error()
     torch.cuda.synchronize()
@@ -45,18 +50,33 @@ def test_tc_gemm(torch_cuda, prec, n, K, N):
 @pytest.mark.parametrize("n,M,N", [(1000, 16, 16), (200001, 16, 16), (65536, 32, 32), (4097, 48, 16), (129, 64, 64),
                                    (50, 16, 48), (777, 12, 5), (3, 1, 16), (99999, 8, 8), (100003, 16, 9)])
 def test_gram(torch_cuda, prec, n, M, N):
+    _gram_case(torch_cuda, prec, n, M, N, M, N)
+
+
+# strided rows and row lengths that are not whole 16-byte units: the
+# pipelined kernel takes rows of up to 64 floats in whole units, the older
+# kernels the rest
+@pytest.mark.parametrize("prec", [_lib.DENSE_BF16, _lib.DENSE_TF32X3])
+@pytest.mark.parametrize("n,M,N,ldx,ldw", [(70001, 16, 16, 20, 32), (5000, 10, 6, 12, 8), (3333, 7, 16, 7, 16),
+                                           (40000, 24, 20, 24, 20), (1000, 16, 16, 100, 16)])
+def test_gram_strided(torch_cuda, prec, n, M, N, ldx, ldw):
+    _gram_case(torch_cuda, prec, n, M, N, ldx, ldw)
+
+
+def _gram_case(torch_cuda, prec, n, M, N, ldx, ldw):
     torch = torch_cuda
     g = torch.Generator(device="cuda").manual_seed(n + M + N)
-    X = torch.randn((n, M), generator=g, device="cuda")
-    W = torch.randn((n, N), generator=g, device="cuda")
+    Xf = torch.randn((n, ldx), generator=g, device="cuda")
+    Wf = torch.randn((n, ldw), generator=g, device="cuda")
+    X, W = Xf[:, :M], Wf[:, :N]
     parts = _lib.lib.fmx_dense_gram_parts(prec, n)
     dt = torch.float64 if prec == _lib.DENSE_F64 else torch.float32
     part = torch.empty(parts * M * N, dtype=dt, device="cuda")
     G = torch.full((M, N), float("nan"), dtype=dt, device="cuda")
     err = torch.zeros(1, dtype=torch.int32, device="cuda")
     for _ in range(2):                      # deterministic: same bits twice
-        rc = _lib.lib.fmx_dense_gram(prec, X.data_ptr(), M, M, W.data_ptr(), N, N, n, part.data_ptr(), G.data_ptr(),
-                                     err.data_ptr(), _stream(torch))
+        rc = _lib.lib.fmx_dense_gram(prec, Xf.data_ptr(), ldx, M, Wf.data_ptr(), ldw, N, n, part.data_ptr(),
+                                     G.data_ptr(), err.data_ptr(), _stream(torch))
         assert rc == 0, _lib.last_error()
         torch.cuda.synchronize()
         if _ == 0:
