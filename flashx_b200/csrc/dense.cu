@@ -310,10 +310,15 @@ tc_gemm_kernel(const float *__restrict__ X, int64_t ldx, int K, const float *__r
 // ---------------------------------------------------------------------------
 // Pipelined tensor-core kernels: Y = X B (GEMM) and part[cta] = X^T W (Gram).
 //
-// Rows of X (and W) stream through shared memory in tiles of 128 rows, one
-// cp.async.bulk copy per tile and matrix (rows of ldx floats, contiguous).
+// Rows of X (and W) stream through shared memory in tiles of 128 rows: each
+// converter thread copies its own row of a tile with 16-byte cp.async copies
+// (through L2, no L1 allocation), kRawStages tiles ahead, into a ring of raw
+// stages, and waits only for its own copies (cp.async.wait_group).  (A
+// single producer thread issuing one cp.async.bulk copy per tile measured
+// about 1,900 cycles per 8 KB tile per SM: the bulk-copy path, not memory,
+// bounded the kernel.)
 // Warp roles (320 threads, one CTA per SM):
-//   warp 0     producer: the bulk copies, into a ring of RS raw stages
+//   warp 0     idle
 //   warp 1     MMA issuer (one lane) and TMEM owner
 //   warps 2-5  converters (thread r owns row r of a tile): raw rows -> MMA
 //              operands in a ring of OS operand stages; 3xTF32 splits
@@ -322,9 +327,8 @@ tc_gemm_kernel(const float *__restrict__ X, int64_t ldx, int K, const float *__r
 //   warps 6-9  GEMM epilogue: TMEM lane quarter (warp % 4) -> Y rows, from a
 //              ring of AS accumulators, so the MMAs of later tiles overlap
 // Barriers (every wait bounded; one that runs out sets *err, and before the
-// CTA exits the producer waits, bounded, for its copies in flight and the
-// MMA lane for its MMAs):
-//   full[i]    copy bytes landed          rfree[i]  converters read the rows
+// CTA exits every converter waits for its copies and the MMA lane for its
+// MMAs):
 //   opr[i]     operands written           opf[i]    the MMAs read them
 //   accf[i]    accumulator complete       acce[i]   epilogue drained it
 // Operand layouts, no swizzle, 16-byte units:
@@ -340,8 +344,6 @@ tc_gemm_kernel(const float *__restrict__ X, int64_t ldx, int K, const float *__r
 //     so the threads' 4-byte stores hit 32 banks; A's 64 rows per K unit
 //     overlap the next unit's rows, which only feeds unread D rows.
 // ---------------------------------------------------------------------------
-constexpr int kPipeRing = 8;
-constexpr int kGemmThreads = 320;
 constexpr size_t kPipeSmemBudget = size_t(200) << 10;   // the rings' target size
 constexpr size_t kPipeSmemMax = size_t(220) << 10;      // at most (227 KB per CTA, less the static part)
 
@@ -360,6 +362,16 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t b
 	asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
 			:: "r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
 }
+// 16-byte asynchronous copy global -> shared through L2 (no L1 allocation);
+// a thread waits for its own copies with cp.async.wait_group.
+__device__ __forceinline__ void cp_async16(void *dst, const void *src)
+{
+	asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" :: "n"(N) : "memory"); }
+
 constexpr uint32_t instr_desc_m64(uint32_t fmt, uint32_t a_mn, uint32_t b_mn, uint32_t n)
 {
 	return (1u << 4) | (fmt << 7) | (fmt << 10) | (a_mn << 15) | (b_mn << 16) | ((n >> 3) << 17) | ((64u >> 4) << 24);
@@ -374,27 +386,32 @@ struct pipe_plan {
 	size_t bpart;                     // GEMM: bytes of one part of B^T
 	size_t tail;                      // bytes the last operand stage's MMA reads past its end
 	int lba, lbb;                     // Gram 3xTF32: K-unit strides of A and B
+	int mh = 0;                       // Gram 3xTF32: first A row of the lo parts
 	size_t a_op, b_op;                // Gram: bytes of A and B operands (one part)
-	int RS, OS, AS;
+	int ru;                           // 16-byte units per raw row
+	int NG, RS, OS, AS;               // converter groups, raw stages per group, operand and accumulator stages
 	size_t smem;
-	__host__ __device__ pipe_plan(bool gram_, bool tf32_, int K_, int N_, int64_t ldx_, int64_t ldw_)
+	__host__ __device__ pipe_plan(bool gram_, bool tf32_, int K_, int N_, int64_t ldx_, int64_t ldw_, int rs_, int ng_)
 		: gram(gram_), tf32(tf32_), K(K_), N(N_), ldx(ldx_), ldw(ldw_)
 	{
 		const int KSTEP = tf32 ? 8 : 16;
 		Kp = (K + KSTEP - 1) / KSTEP * KSTEP;
 		Np = (N + 15) / 16 * 16;
-		raw = size_t(kTile) * 4 * size_t(ldx + (gram ? ldw : 0));
+		ru = (K + 3) / 4 + (gram ? (N + 3) / 4 : 0);      // 16-byte units of a raw row
+		raw = size_t(kTile) * 16 * size_t(ru);
 		bpart = 0; tail = 0; lba = lbb = 0; a_op = b_op = 0;
 		if (!gram) {
 			const size_t part = tf32 ? size_t(Kp / 4) * kTile * 16 : size_t(Kp / 8) * kTile * 16;
 			op = (tf32 ? 2 : 1) * part;
 			bpart = tf32 ? size_t(Kp / 4) * Np * 16 : size_t(Kp / 8) * Np * 16;
 		} else if (tf32) {
-			lba = (K + 7) / 8 * 128 + 16;
-			lbb = Np * 16 + 16;
+			// A rows: X hi at 0.., X lo at mh..; B rows: W hi at 0.., W lo at Np..
+			mh = K <= 16 ? 16 : 32;
+			lba = 2 * mh * 16 + 16;
+			lbb = 2 * Np * 16 + 16;
 			a_op = size_t(kTile / 4) * lba;
 			b_op = size_t(kTile / 4) * lbb;
-			op = 2 * (a_op + b_op);
+			op = a_op + b_op;
 			// A's last K unit is read for 64 rows
 			tail = size_t(64 * 16) > size_t(lba) ? size_t(64 * 16 - lba) : 0;
 		} else {
@@ -404,37 +421,39 @@ struct pipe_plan {
 			tail = size_t(8) * kTile * 16 > a_op ? size_t(8) * kTile * 16 - a_op : 0;
 		}
 		AS = gram ? 1 : (Np <= 32 ? 8 : (Np <= 64 ? 4 : 2));
-		acc_cols = gram ? (Np <= 32 ? 32 : 64) : size_t(AS) * Np;
+		acc_cols = gram ? size_t((tf32 ? 2 : 1) * Np) : size_t(AS) * Np;
 		if (acc_cols < 32) acc_cols = 32;
-		// operand stages: 4 when they are small, else 2 (the raw stages carry
-		// the loads in flight); raw stages: as many as fit, up to the ring size
+		// raw stages: RS tiles in flight per converter thread, NG groups;
+		// operand stages: two per group when they fit, else one
 		const size_t fixed = 2 * bpart + tail;
-		OS = (op <= 16384 && fixed + 4 * op + 6 * raw <= kPipeSmemBudget) ? 4 : 2;
-		RS = 2;
-		const size_t left = kPipeSmemBudget > fixed + size_t(OS) * op ? kPipeSmemBudget - fixed - size_t(OS) * op : 0;
-		RS = int(left / raw);
-		if (RS > kPipeRing) RS = kPipeRing;
-		if (RS < 2) RS = 2;
-		smem = size_t(RS) * raw + size_t(OS) * op + 2 * bpart + tail;
+		NG = ng_;
+		RS = rs_;
+		OS = fixed + size_t(2 * NG) * op + size_t(NG * RS) * raw <= kPipeSmemBudget ? 2 * NG : NG;
+		smem = size_t(NG * RS) * raw + size_t(OS) * op + 2 * bpart + tail;
 	}
 	__host__ __device__ bool fits() const { return smem <= kPipeSmemMax; }
 };
 
-template <bool TF32, bool GRAM>
-__global__ void __launch_bounds__(kGemmThreads, 1)
+// threads of a CTA with NG converter groups: warp 0 (idle), warp 1 (MMA), NG
+// groups of 4 converter warps, 4 epilogue warps
+constexpr int pipe_threads(int ng) { return 32 * (6 + 4 * ng); }
+
+template <bool TF32, bool GRAM, int kRawStages, int NGROUPS>
+__global__ void __launch_bounds__(pipe_threads(NGROUPS), 1)
 tc_pipe_kernel(const float *__restrict__ X, int64_t ldx, int K, const float *__restrict__ Wm, int64_t ldw, int N,
 		const float *__restrict__ B, int ldb, float *__restrict__ Y, int64_t ldy, float *__restrict__ part, int64_t n,
 		int *err)
 {
-	const pipe_plan P(GRAM, TF32, K, N, ldx, ldw);
+	const pipe_plan P(GRAM, TF32, K, N, ldx, ldw, kRawStages, NGROUPS);
 	constexpr int KSTEP = TF32 ? 8 : 16;
 	const int Kp = P.Kp, Np = P.Np, RS = P.RS, OS = P.OS, AS = P.AS;
 	extern __shared__ __align__(1024) char smem[];
 	// layout: raw ring, operand ring (plus the tail the last one reads), B^T
 	char *raw0 = smem;
-	char *op0 = smem + size_t(RS) * P.raw;
+	char *op0 = smem + size_t(NGROUPS * RS) * P.raw;
 	char *sb = op0 + size_t(OS) * P.op + P.tail;
-	__shared__ uint64_t full[kPipeRing], rfree[kPipeRing], opr[4], opf[4], accf[8], acce[8];
+	__shared__ uint64_t opr[2 * NGROUPS], opf[2 * NGROUPS], accf[8], acce[8];
+	constexpr int kEpi0 = 2 + 4 * NGROUPS;             // first epilogue warp
 	__shared__ uint32_t tmem_base;
 	__shared__ int bad;
 	const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -451,7 +470,6 @@ tc_pipe_kernel(const float *__restrict__ X, int64_t ldx, int K, const float *__r
 	}
 	if (warp == 1) tmem_alloc(&tmem_base, ncols);
 	if (tid == 0) {
-		for (int i = 0; i < RS; i++) { mbar_init(&full[i], 1); mbar_init(&rfree[i], 4); }
 		for (int i = 0; i < OS; i++) { mbar_init(&opr[i], 4); mbar_init(&opf[i], 1); }
 		for (int i = 0; i < AS; i++) { mbar_init(&accf[i], 1); mbar_init(&acce[i], 4); }
 		bad = 0;
@@ -466,37 +484,19 @@ tc_pipe_kernel(const float *__restrict__ X, int64_t ldx, int K, const float *__r
 	const int64_t my_tiles = int64_t(blockIdx.x) < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
 	bool ok = true;
 	auto tile_row = [&](int64_t i) { return (int64_t(blockIdx.x) + i * int64_t(gridDim.x)) * kTile; };
-	// operand stage o: GEMM: part 1 (hi / BF16), part 2 (lo); Gram: A1 [A2] B1 [B2]
+	// operand stage o: GEMM: part 1 (hi / BF16), part 2 (lo); Gram: A then B
 	auto OPA1 = [&](int o) { return op0 + size_t(o) * P.op; };
-	auto OPA2 = [&](int o) { return OPA1(o) + (GRAM ? P.a_op : P.op / 2); };
-	auto OPB1 = [&](int o) { return OPA1(o) + (TF32 ? 2 : 1) * P.a_op; };
-	auto OPB2 = [&](int o) { return OPB1(o) + P.b_op; };
+	auto OPA2 = [&](int o) { return OPA1(o) + P.op / 2; };    // GEMM 3xTF32: the lo part
+	auto OPB1 = [&](int o) { return OPA1(o) + P.a_op; };
 
 	if (warp == 0) {
-		// ---- producer ----
-		if (lane == 0) {
-			int64_t issued = 0;
-			for (int64_t i = 0; i < my_tiles && ok; i++) {
-				const int s = int(i % RS);
-				if (i >= RS && !mbar_wait(&rfree[s], uint32_t((i / RS - 1) & 1))) { ok = false; break; }
-				const int64_t r0 = tile_row(i);
-				const int64_t rows = std::min<int64_t>(kTile, n - r0);
-				const uint32_t bx = uint32_t(rows * ldx * 4), bw = GRAM ? uint32_t(rows * ldw * 4) : 0u;
-				char *dst = raw0 + size_t(s) * P.raw;
-				mbar_expect_tx(&full[s], bx + bw);
-				bulk_load(dst, X + r0 * ldx, bx, &full[s]);
-				if (GRAM) bulk_load(dst + size_t(kTile) * 4 * size_t(ldx), Wm + r0 * ldw, bw, &full[s]);
-				issued = i + 1;
-			}
-			// copies still in flight must land before the CTA may exit
-			for (int64_t j = std::max<int64_t>(0, issued - RS); j < issued; j++)
-				if (!mbar_wait(&full[j % RS], uint32_t((j / RS) & 1))) ok = false;
-		}
+		// idle
 	} else if (warp == 1) {
 		// ---- MMA issuer ----
 		if (lane == 0) {
 			uint32_t idesc;
-			if constexpr (GRAM) idesc = TF32 ? instr_desc_m64(2, 0, 0, uint32_t(Np)) : instr_desc_m64(1, 1, 1, uint32_t(Np));
+			// the 3xTF32 Gram stacks hi and lo: D = [X hi; X lo]^T-rows x [W hi, W lo]
+			if constexpr (GRAM) idesc = TF32 ? instr_desc_m64(2, 0, 0, uint32_t(2 * Np)) : instr_desc_m64(1, 1, 1, uint32_t(Np));
 			else idesc = instr_desc(TF32 ? 2 : 1, 0, 0, uint32_t(Np));
 			// descriptors once: the start address is the low field (16-byte
 			// units), so an operand at byte offset `off` from the base is the
@@ -512,11 +512,9 @@ tc_pipe_kernel(const float *__restrict__ X, int64_t ldx, int K, const float *__r
 				b_pass1 = uint32_t(P.bpart / 16);
 			} else if constexpr (TF32) {
 				dA = smem_desc(smem_u32(op0), P.lba, 128);
-				dB = smem_desc(smem_u32(op0) + uint32_t(2 * P.a_op), P.lbb, 128);
+				dB = smem_desc(smem_u32(op0) + uint32_t(P.a_op), P.lbb, 128);
 				a_step = 2 * P.lba / 16;
 				b_step = 2 * P.lbb / 16;
-				a_pass2 = uint32_t(P.a_op / 16);
-				b_pass1 = uint32_t(P.b_op / 16);
 			} else {
 				dA = smem_desc(smem_u32(op0), 128, kTile * 16);
 				dB = smem_desc(smem_u32(op0) + uint32_t(P.a_op), 128, kTile * 16);
@@ -533,8 +531,8 @@ tc_pipe_kernel(const float *__restrict__ X, int64_t ldx, int K, const float *__r
 				const uint64_t stage_off = uint64_t(o) * (P.op / 16);
 				const uint32_t d = GRAM ? tmem : tmem + uint32_t(b * Np);
 				if constexpr (!GRAM) acc = 0;
-				for (int pass = 0; pass < (TF32 ? 3 : 1); pass++) {
-					// (hi, hi), (hi, lo), (lo, hi)
+				for (int pass = 0; pass < ((TF32 && !GRAM) ? 3 : 1); pass++) {
+					// GEMM: (hi, hi), (hi, lo), (lo, hi); Gram: all in one
 					uint64_t a = dA + stage_off + (pass == 2 ? a_pass2 : 0);
 					uint64_t bd = dB + (GRAM ? stage_off : 0) + (pass == 1 ? b_pass1 : 0);
 					for (int ks = 0; ks < nks; ks++) {
@@ -555,25 +553,48 @@ tc_pipe_kernel(const float *__restrict__ X, int64_t ldx, int K, const float *__r
 				if (issued && !mbar_wait(&accf[(issued - 1) % AS], uint32_t(((issued - 1) / AS) & 1))) ok = false;
 			}
 		}
-	} else if (warp < 6) {
-		// ---- converters ----
-		const int r = tid - 64;
-		for (int64_t i = 0; i < my_tiles && ok; i++) {
-			const int s = int(i % RS), o = int(i % OS);
-			if (!mbar_wait(&full[s], uint32_t((i / RS) & 1))) { ok = false; break; }
+	} else if (warp < kEpi0) {
+		// ---- converters: group g takes tiles g, g + NG, ...; its thread r
+		// copies and converts row r of each ----
+		const int g = (warp - 2) / 4;
+		const int r = tid - 64 - 128 * g;
+		const int xu = (K + 3) / 4, wu = GRAM ? (N + 3) / 4 : 0;
+		auto row_of = [&](int st) {
+			return raw0 + size_t(g * RS + st) * P.raw + size_t(r) * size_t(P.ru) * 16;
+		};
+		// local tile j of the group is tile g + j NG of the CTA
+		auto issue = [&](int64_t j) {
+			const int64_t i = g + j * NGROUPS;
+			if (i < my_tiles) {
+				const int64_t row = tile_row(i) + r;
+				if (row < n) {
+					char *d = row_of(int(j % RS));
+					const float *sx = X + row * ldx;
+					for (int u = 0; u < xu; u++) cp_async16(d + 16 * u, sx + 4 * u);
+					if (GRAM) {
+						const float *sw = Wm + row * ldw;
+						for (int u = 0; u < wu; u++) cp_async16(d + 16 * (xu + u), sw + 4 * u);
+					}
+				}
+			}
+			cp_async_commit();                        // one group per tile (empty past the end)
+		};
+		for (int j = 0; j < kRawStages - 1; j++) issue(j);
+		for (int64_t j = 0, i = g; i < my_tiles && ok; j++, i += NGROUPS) {
+			const int s = int(j % RS), o = int(i % OS);
+			issue(j + kRawStages - 1);                    // into the stage read in the last iteration
+			cp_async_wait<kRawStages - 1>();              // this thread's copies of tile i have landed
 			if (i >= OS && !mbar_wait(&opf[o], uint32_t((i / OS - 1) & 1))) { ok = false; break; }
 			const bool live = tile_row(i) + r < n;
-			const char *rs = raw0 + size_t(s) * P.raw;
 			for (int side = 0; side < (GRAM ? 2 : 1); side++) {
 				const int L = side ? N : K;
-				const int64_t ld = side ? ldw : ldx;
-				const float *xr = reinterpret_cast<const float *>(rs + (side ? size_t(kTile) * 4 * size_t(ldx) : 0) +
-						size_t(r) * size_t(ld) * 4);
+				const float *xr = reinterpret_cast<const float *>(row_of(s) + (side ? size_t(xu) * 16 : 0));
 				if (TF32 && GRAM) {
 					// K-major transpose (4-byte stores, 32 banks per warp)
-					char *o1 = side ? OPB1(o) : OPA1(o), *o2 = side ? OPB2(o) : OPA2(o);
+					char *o1 = side ? OPB1(o) : OPA1(o);
 					const int lb = side ? P.lbb : P.lba;
-					char *b1 = o1 + size_t(r / 4) * lb + (r % 4) * 4, *b2 = o2 + size_t(r / 4) * lb + (r % 4) * 4;
+					char *b1 = o1 + size_t(r / 4) * lb + (r % 4) * 4;
+					char *b2 = b1 + size_t(side ? Np : P.mh) * 16;      // the lo rows
 					const int units = (L + 3) / 4;
 					int u = r % units;                   // rotated start: the reads of a wavefront spread over banks
 					for (int u0 = 0; u0 < units; u0++, u = (u + 1 == units) ? 0 : u + 1) {
@@ -599,32 +620,23 @@ tc_pipe_kernel(const float *__restrict__ X, int64_t ldx, int K, const float *__r
 						}
 					}
 				} else if (TF32) {
-					// GEMM, K-major units of 4: hi and lo; the row's loads go first
+					// GEMM, K-major units of 4: hi and lo
 					char *o1 = OPA1(o), *o2 = OPA2(o);
 					const int units = K / 4;
-					float4 xv[16];
-					const int rot = r % units;           // rotated start: a wavefront's reads spread over banks
+					int u = r % units;                   // rotated start: a wavefront's reads spread over banks
+					for (int u0 = 0; u0 < units; u0++, u = (u + 1 == units) ? 0 : u + 1) {
+						const float4 x = live ? reinterpret_cast<const float4 *>(xr)[u] : make_float4(0.f, 0.f, 0.f, 0.f);
+						const uint32_t xs[4] = {__float_as_uint(x.x), __float_as_uint(x.y), __float_as_uint(x.z),
+								__float_as_uint(x.w)};
+						uint32_t hi[4], lo[4];
 #pragma unroll
-					for (int u0 = 0; u0 < 16; u0++)
-						if (u0 < units) {
-							const int u = u0 + rot < units ? u0 + rot : u0 + rot - units;
-							xv[u0] = live ? reinterpret_cast<const float4 *>(xr)[u] : make_float4(0.f, 0.f, 0.f, 0.f);
+						for (int q = 0; q < 4; q++) {
+							hi[q] = xs[q] & 0xFFFFE000u;
+							lo[q] = __float_as_uint(__fsub_rn(__uint_as_float(xs[q]), __uint_as_float(hi[q])));
 						}
-#pragma unroll
-					for (int u0 = 0; u0 < 16; u0++)
-						if (u0 < units) {
-							const int u = u0 + rot < units ? u0 + rot : u0 + rot - units;
-							const uint32_t xs[4] = {__float_as_uint(xv[u0].x), __float_as_uint(xv[u0].y),
-									__float_as_uint(xv[u0].z), __float_as_uint(xv[u0].w)};
-							uint32_t hi[4], lo[4];
-#pragma unroll
-							for (int q = 0; q < 4; q++) {
-								hi[q] = xs[q] & 0xFFFFE000u;
-								lo[q] = __float_as_uint(__fsub_rn(__uint_as_float(xs[q]), __uint_as_float(hi[q])));
-							}
-							*reinterpret_cast<uint4 *>(o1 + size_t(u) * kTile * 16 + size_t(r) * 16) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-							*reinterpret_cast<uint4 *>(o2 + size_t(u) * kTile * 16 + size_t(r) * 16) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
-						}
+						*reinterpret_cast<uint4 *>(o1 + size_t(u) * kTile * 16 + size_t(r) * 16) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+						*reinterpret_cast<uint4 *>(o2 + size_t(u) * kTile * 16 + size_t(r) * 16) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+					}
 				} else {
 					// BF16 units of 8 (GEMM K-major, Gram MN-major: the same writes)
 					char *o1 = GRAM ? (side ? OPB1(o) : OPA1(o)) : OPA1(o);
@@ -653,9 +665,10 @@ tc_pipe_kernel(const float *__restrict__ X, int64_t ldx, int K, const float *__r
 			}
 			fence_async_smem();
 			__syncwarp();
-			if (lane == 0) { mbar_arrive(&rfree[s]); mbar_arrive(&opr[o]); }
+			if (lane == 0) mbar_arrive(&opr[o]);
 		}
-		if constexpr (GRAM) {
+		cp_async_wait<0>();                               // no copy in flight when the CTA exits
+		if (GRAM && g == 0) {
 			// read out D: warp quarter q holds rows 16 q .. 16 q + 15 in lanes 32 q .. 32 q + 15
 			const bool done = ok && mbar_wait(&accf[0], 0);
 			const bool all = __all_sync(0xffffffffu, done);
@@ -663,13 +676,29 @@ tc_pipe_kernel(const float *__restrict__ X, int64_t ldx, int K, const float *__r
 			if (all) {
 				tc_fence_after();
 				const int q = warp & 3;
-				const int m = 16 * q + lane;
-				for (int c0 = 0; c0 < Np; c0 += 16) {
-					float o[16];
-					tmem_ld16(tmem + (uint32_t(q * 32) << 16) + uint32_t(c0), o);
-					if (lane < 16 && m < K)
-						for (int c = 0; c < 16 && c0 + c < N; c++)
-							part[(size_t(blockIdx.x) * K + m) * N + c0 + c] = my_tiles ? o[c] : 0.f;
+				const int dm = 16 * q + lane;                  // the D row of this lane (lane < 16)
+				if constexpr (TF32) {
+					// two partials per CTA: rows < mh give hi W hi + hi W lo, rows
+					// >= mh give lo W hi
+					const bool hi_row = dm < P.mh;
+					const int m = hi_row ? dm : dm - P.mh;
+					float *pp = part + (size_t(2 * blockIdx.x) + (hi_row ? 0 : 1)) * K * N;
+					for (int c0 = 0; c0 < Np; c0 += 16) {
+						float o[16], o2[16];
+						tmem_ld16(tmem + (uint32_t(q * 32) << 16) + uint32_t(c0), o);
+						tmem_ld16(tmem + (uint32_t(q * 32) << 16) + uint32_t(Np + c0), o2);
+						if (lane < 16 && m < K)
+							for (int c = 0; c < 16 && c0 + c < N; c++)
+								pp[size_t(m) * N + c0 + c] = my_tiles ? (hi_row ? __fadd_rn(o[c], o2[c]) : o[c]) : 0.f;
+					}
+				} else {
+					for (int c0 = 0; c0 < Np; c0 += 16) {
+						float o[16];
+						tmem_ld16(tmem + (uint32_t(q * 32) << 16) + uint32_t(c0), o);
+						if (lane < 16 && dm < K)
+							for (int c = 0; c < 16 && c0 + c < N; c++)
+								part[(size_t(blockIdx.x) * K + dm) * N + c0 + c] = my_tiles ? o[c] : 0.f;
+					}
 				}
 			}
 		}
@@ -1197,12 +1226,17 @@ int fmx_dense_gemm(int precision, const float *X, int64_t ldx, int64_t n, int K,
 	// the pipelined kernel when the rows of X can be bulk-copied (16-byte
 	// aligned rows of whole 16-byte units)
 	if (K % 4 == 0 && ldx % 4 == 0 && ldx <= 64 && (reinterpret_cast<uintptr_t>(X) & 15) == 0 && n > 0) {
-		const pipe_plan P(false, tf32, K, N, ldx, 0);
-		if (P.fits()) {
-			auto kern = tf32 ? tc_pipe_kernel<true, false> : tc_pipe_kernel<false, false>;
+		// four converter groups when they fit, else two, else one
+		const pipe_plan P4(false, tf32, K, N, ldx, 0, 3, 4), P2(false, tf32, K, N, ldx, 0, 3, 2),
+				P1(false, tf32, K, N, ldx, 0, 3, 1);
+		if (P4.fits() || P2.fits() || P1.fits()) {
+			const pipe_plan &P = P4.fits() ? P4 : (P2.fits() ? P2 : P1);
+			auto kern = P4.fits() ? (tf32 ? tc_pipe_kernel<true, false, 3, 4> : tc_pipe_kernel<false, false, 3, 4>)
+			          : P2.fits() ? (tf32 ? tc_pipe_kernel<true, false, 3, 2> : tc_pipe_kernel<false, false, 3, 2>)
+			                      : (tf32 ? tc_pipe_kernel<true, false, 3, 1> : tc_pipe_kernel<false, false, 3, 1>);
 			DCUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(P.smem)));
 			const unsigned grid = unsigned(std::max<int64_t>(1, std::min<int64_t>(tiles, int64_t(sms(dev)))));
-			kern<<<grid, kGemmThreads, P.smem, st>>>(X, ldx, K, nullptr, 0, N, B, ldb, Y, ldy, nullptr, n, err);
+			kern<<<grid, pipe_threads(P.NG), P.smem, st>>>(X, ldx, K, nullptr, 0, N, B, ldb, Y, ldy, nullptr, n, err);
 			DCUDA_TRY(cudaGetLastError());
 			return FMX_OK;
 		}
@@ -1228,9 +1262,10 @@ int fmx_dense_gram_parts(int precision, int64_t n)
 	cudaGetDevice(&dev);
 	const int64_t chunks = (n + kTile - 1) / kTile;
 	if (precision == FMX_DENSE_F64) return int(std::max<int64_t>(1, std::min<int64_t>((n + 63) / 64, int64_t(sms(dev)) * 4)));
-	return int(std::max<int64_t>(1, std::min<int64_t>(chunks, int64_t(sms(dev)) * (precision == FMX_DENSE_TF32X3 ? 1 : 2))));
-	// (the pipelined tensor-core Gram runs one CTA per SM, the older kernel up
-	// to two: callers size their partials with this count either way)
+	// tensor cores: one CTA per SM; the pipelined 3xTF32 kernel leaves two
+	// partials per CTA (the older kernels launch one CTA per partial)
+	const int ctas = int(std::max<int64_t>(1, std::min<int64_t>(chunks, int64_t(sms(dev)))));
+	return precision == FMX_DENSE_TF32X3 ? 2 * ctas : ctas;
 }
 
 int fmx_dense_gram(int precision, const float *X, int64_t ldx, int M, const float *W, int64_t ldw, int N, int64_t n,
@@ -1255,13 +1290,18 @@ int fmx_dense_gram(int precision, const float *X, int64_t ldx, int M, const floa
 	const bool tf32 = precision == FMX_DENSE_TF32X3;
 	if (!tf32 && precision != FMX_DENSE_BF16) return set_error(FMX_ERR_INVAL, "unknown precision %d", precision);
 	if (ldx % 4 == 0 && ldw % 4 == 0 && ldx <= 64 && ldw <= 64 && (reinterpret_cast<uintptr_t>(X) & 15) == 0 &&
-			(reinterpret_cast<uintptr_t>(W) & 15) == 0 && n > 0) {
-		const pipe_plan P(true, tf32, M, N, ldx, ldw);
-		if (P.fits()) {
+			(reinterpret_cast<uintptr_t>(W) & 15) == 0 && n > 0 && (!tf32 || M <= 32)) {
+		const pipe_plan P4(true, tf32, M, N, ldx, ldw, 3, 4), P2(true, tf32, M, N, ldx, ldw, 3, 2),
+				P1(true, tf32, M, N, ldx, ldw, 3, 1);
+		if (P4.fits() || P2.fits() || P1.fits()) {
 			// the pipelined kernel: one CTA per SM, partials reduced in CTA order
-			auto kern = tf32 ? tc_pipe_kernel<true, true> : tc_pipe_kernel<false, true>;
+			const pipe_plan &P = P4.fits() ? P4 : (P2.fits() ? P2 : P1);
+			auto kern = P4.fits() ? (tf32 ? tc_pipe_kernel<true, true, 3, 4> : tc_pipe_kernel<false, true, 3, 4>)
+			          : P2.fits() ? (tf32 ? tc_pipe_kernel<true, true, 3, 2> : tc_pipe_kernel<false, true, 3, 2>)
+			                      : (tf32 ? tc_pipe_kernel<true, true, 3, 1> : tc_pipe_kernel<false, true, 3, 1>);
 			DCUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(P.smem)));
-			kern<<<parts, kGemmThreads, P.smem, st>>>(X, ldx, M, W, ldw, N, nullptr, 0, nullptr, 0,
+			// the 3xTF32 kernel leaves two partials per CTA
+			kern<<<tf32 ? parts / 2 : parts, pipe_threads(P.NG), P.smem, st>>>(X, ldx, M, W, ldw, N, nullptr, 0, nullptr, 0,
 					static_cast<float *>(part), n, err);
 			DCUDA_TRY(cudaGetLastError());
 			gram_reduce_kernel<float><<<(M * N + 7) / 8, 256, 0, st>>>(static_cast<const float *>(part), parts, M * N,

@@ -1549,7 +1549,10 @@ static int run_typed(const gpu_part &p, const void *X, int64_t ldx, void *Y, int
 		int rc;
 		// 32-byte lanes: FP32 accumulation, a panel of whole 32-byte lanes,
 		// X, Y and the packed rows 32-byte aligned
-		const bool wide = std::is_same<A, float>::value && vec_ok && (kp * sizeof(XT)) % 32 == 0 &&
+		// (BF16 rows of 16 elements take the 16-byte lanes: measured at R-MAT
+		// scale 24, k = 16, one 32-byte lane per row loads an index group per
+		// lane and ran 2.2 ms against 1.8 ms)
+		const bool wide = std::is_same<A, float>::value && sizeof(XT) == 4 && vec_ok && (kp * sizeof(XT)) % 32 == 0 &&
 				(ldx * sizeof(XT)) % 32 == 0 && (ldy * sizeof(YT)) % 32 == 0 && aligned32(a.X) && aligned32(a.Y);
 		if (wide) {
 			a.G = int(kp * sizeof(XT) / 32);     // 1, 2 or 4
