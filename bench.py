@@ -66,6 +66,13 @@ def parse():
     p.add_argument("--large", action="store_true",
                    help="run only the large single-GPU configuration (R-MAT scale 26: SpMM k=16 and 32, top-16 "
                         "eigensolve plain / mixed / learned start) and print its JSON line")
+    p.add_argument("--skip-sweep", action="store_true")
+    p.add_argument("--skip-dense", action="store_true")
+    p.add_argument("--dense-only", action="store_true",
+                   help="run only the eigensolver's dense tensor-core kernels (n = 2^22, 16 columns) and print "
+                        "their JSON object")
+    p.add_argument("--skip-large", action="store_true")
+    p.add_argument("--large-scale", type=int, default=26)
     return p.parse_args()
 
 
@@ -523,69 +530,169 @@ def pagerank_measure(a, dev):
     return out
 
 
-def large_run(a):
-    """The large single-GPU configuration: R-MAT scale 26 (edge factor 16,
-    seed 1, deduplicated; int32 column ids), FP32 SpMM at k = 16 and 32 on
-    the directed graph, then the top 16 eigenpairs of D^-1/2 A D^-1/2 of the
-    symmetrised graph (block 24, residual 1e-6): plain, mixed, and mixed from
-    the learned start."""
-    import torch
-    from flashx_b200 import matrix_image, sparse_matrix
-    from flashx_b200.eigen import NA_operator, compute_eigen
-    from flashx_b200.graphs import rmat_edges, symmetrize
-    from flashx_b200 import warmstart as ws
-    dev = torch.device("cuda", 0)
-    scale = 26
-    n = 1 << scale
-    out = {"workload": f"rmat-s{scale}-ef16", "n": n}
-    t = time.time()
-    s, d = rmat_edges(scale, seed=1)
-    img = matrix_image.build(s, d, None, nrows=n, ncols=n, block_size=(16384, 16384), dedup=True)
-    out["directed_build_s"] = round(time.time() - t, 1)
-    t = time.time()
-    m = sparse_matrix.create(img, None)
+def _time_spmm(torch, m, X, Y, steps, warmup=3):
+    """Mean device time (ms) of `steps` fmx_spmm calls after `warmup`."""
+    for _ in range(warmup):
+        m.multiply(X, Y)
     torch.cuda.synchronize()
-    out["create_s"] = round(time.time() - t, 1)
-    nnz = m.get_nnz()
-    out["directed_nnz"] = int(nnz)
-    del img
-    for k in (16, 32):
-        X = torch.randn((n, k), device=dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        m.multiply(X, Y)
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def sweep_measure(a, m, n, nnz, dev, peak, steps=20):
+    """The GPU SpMM sweep of the configuration at the bench's scale: k = 1, 4
+    and 32 on the bench matrix (unweighted, FP32 X ~ N(0,1)), and k = 16 on
+    the same R-MAT graph with uniform(0,1] FP32 weights (built on the GPU
+    from the device R-MAT stream)."""
+    import torch
+    from flashx_b200 import sparse_matrix
+    from flashx_b200.graphs import rmat_edges_device
+    g = torch.Generator(device=dev).manual_seed(4321)
+    out = {"steps": steps, "timing": "mean of the steps after 3 warm-up calls, CUDA events"}
+
+    def line(ms, k, weighted, nnz_):
+        bb = b_alg(n, n, nnz_, k, weighted)
+        return {"ms": round(ms, 4), "gbs": round(bb / ms / 1e6, 1), "frac": round(bb / ms / 1e6 / peak, 4),
+                "bytes_alg": bb}
+    for k in (1, 4, 32):
+        X = torch.randn((n, k), generator=g, device=dev)
         Y = torch.empty((n, k), device=dev)
-        for _ in range(5):
-            m.multiply(X, Y)
+        out[f"k{k}"] = line(_time_spmm(torch, m, X, Y, steps), k, False, nnz)
+        del X, Y
+    src, dst = rmat_edges_device(a.scale, seed=1, permute=not a.no_permute, device=dev.index)
+    vals = 1.0 - torch.rand(src.shape, generator=g, device=dev)            # (0, 1]
+    t = time.time()
+    mw = sparse_matrix.from_device_edges(src, dst, vals, nrows=n, ncols=n, dedup=True)
+    build_s = time.time() - t
+    del src, dst, vals
+    X = torch.randn((n, 16), generator=g, device=dev)
+    Y = torch.empty((n, 16), device=dev)
+    out["k16_weighted"] = line(_time_spmm(torch, mw, X, Y, steps), 16, True, mw.get_nnz())
+    out["k16_weighted"]["device_build_s"] = round(build_s, 2)
+    del mw, X, Y
+    torch.cuda.empty_cache()
+    return out
+
+
+def dense_measure(dev, peak, n=1 << 22, b=16, steps=20):
+    """The block eigensolver's dense products on the tensor cores and in
+    FP64, on tall-skinny FP32 operands (n rows, b columns): Y = X B (basis
+    update) and G = X^T W (Gram).  Bytes per call: n (K + N) 4; the bound is
+    the measured HBM copy rate."""
+    import torch
+    from flashx_b200 import _lib
+    g = torch.Generator(device=dev).manual_seed(5)
+    X = torch.randn((n, b), generator=g, device=dev)
+    W = torch.randn((n, b), generator=g, device=dev)
+    B = torch.randn((b, b), generator=g, device=dev)
+    Y = torch.empty((n, b), device=dev)
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    st = torch.cuda.current_stream(dev).cuda_stream
+    out = {"n": n, "columns": b, "bytes_per_call": n * 2 * b * 4,
+           "timing": f"mean of {steps} calls after 3, CUDA events", "memory_bound_us": round(n * 2 * b * 4 / peak / 1e3, 1)}
+
+    def timed(fn):
+        for _ in range(3):
+            if fn():
+                raise RuntimeError(_lib.last_error())
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        for _ in range(50):
-            m.multiply(X, Y)
+        for _ in range(steps):
+            fn()
         e1.record()
         torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / 50
-        out[f"spmm_k{k}"] = {"ms": round(ms, 3), "gbs": round(b_alg(n, n, nnz, k, False) / ms / 1e6, 1)}
+        return e0.elapsed_time(e1) / steps * 1e3
+    names = {_lib.DENSE_BF16: "bf16", _lib.DENSE_TF32X3: "tf32x3", _lib.DENSE_F64: "f64"}
+    for prec in (_lib.DENSE_TF32X3, _lib.DENSE_BF16):
+        us = timed(lambda: _lib.lib.fmx_dense_gemm(prec, X.data_ptr(), b, n, b, B.data_ptr(), b, b, Y.data_ptr(), b,
+                                                   err.data_ptr(), st))
+        ref = X.double() @ B.double()
+        out[f"gemm_{names[prec]}"] = {"us": round(us, 1), "frac": round(n * 2 * b * 4 / us / 1e3 / peak, 4),
+                                     "rel_err": float(f"{float((Y.double() - ref).abs().max() / ref.abs().max()):.2e}")}
+    ref = X.double().T @ W.double()
+    for prec in (_lib.DENSE_TF32X3, _lib.DENSE_BF16, _lib.DENSE_F64):
+        parts = _lib.lib.fmx_dense_gram_parts(prec, n)
+        dt = torch.float64 if prec == _lib.DENSE_F64 else torch.float32
+        part = torch.empty(parts * b * b, dtype=dt, device=dev)
+        G = torch.empty((b, b), dtype=dt, device=dev)
+        us = timed(lambda: _lib.lib.fmx_dense_gram(prec, X.data_ptr(), b, b, W.data_ptr(), b, b, n, part.data_ptr(),
+                                                   G.data_ptr(), err.data_ptr(), st))
+        out[f"gram_{names[prec]}"] = {"us": round(us, 1), "frac": round(n * 2 * b * 4 / us / 1e3 / peak, 4),
+                                     "rel_err": float(f"{float((G.double() - ref).abs().max() / ref.abs().max()):.2e}")}
+    out["tensor_core_errors"] = int(err.item())
+    del X, W, B, Y
+    torch.cuda.empty_cache()
+    return out
+
+
+def large_measure(a, dev, peak):
+    """The large single-GPU configuration: R-MAT at --large-scale (26: 67M
+    vertices, edge factor 16, seed 1, deduplicated, int32 column ids),
+    generated and built on the GPU; FP32 SpMM at k = 16 and 32 on the
+    directed graph, then the top 16 eigenpairs of D^-1/2 A D^-1/2 of the
+    symmetrised graph (block 24, residual 1e-6): plain, mixed, and mixed from
+    the learned start (one warm-up solve, then one timed solve each)."""
+    import torch
+    from flashx_b200 import sparse_matrix
+    from flashx_b200.eigen import NA_operator, compute_eigen
+    from flashx_b200.graphs import rmat_edges_device
+    from flashx_b200 import warmstart as ws
+    scale = a.large_scale
+    n = 1 << scale
+    out = {"workload": f"rmat-s{scale}-ef16", "n": n, "built": "device R-MAT stream + fmx_matrix_build_device"}
+    src, dst = rmat_edges_device(scale, seed=1, device=dev.index)
+    t = time.time()
+    m = sparse_matrix.from_device_edges(src, dst, None, nrows=n, ncols=n, dedup=True)
+    torch.cuda.synchronize()
+    out["directed_build_s"] = round(time.time() - t, 1)
+    nnz = m.get_nnz()
+    out["directed_nnz"] = int(nnz)
+    g = torch.Generator(device=dev).manual_seed(99)
+    for k in (16, 32):
+        X = torch.randn((n, k), generator=g, device=dev)
+        Y = torch.empty((n, k), device=dev)
+        ms = _time_spmm(torch, m, X, Y, 10)
+        bb = b_alg(n, n, nnz, k, False)
+        out[f"spmm_k{k}"] = {"ms": round(ms, 3), "gbs": round(bb / ms / 1e6, 1), "frac": round(bb / ms / 1e6 / peak, 4)}
         del X, Y
     del m
     torch.cuda.empty_cache()
     t = time.time()
-    s, d = symmetrize(s, d)
-    img = matrix_image.build(s, d, None, nrows=n, ncols=n, block_size=(16384, 16384), dedup=True)
-    del s, d
-    m = sparse_matrix.create(img, None)
-    del img
-    op = NA_operator(m)
+    # both directions of every edge; self-loops go first (the builder drops
+    # them anyway), which keeps the list under the builder's 2^31 edges
+    keep = src != dst
+    src, dst = src[keep], dst[keep]
+    del keep
+    ssym = torch.cat([src, dst])
+    dsym = torch.cat([dst, src])
+    del src, dst
+    m = sparse_matrix.from_device_edges(ssym, dsym, None, nrows=n, ncols=n, dedup=True)
+    del ssym, dsym
+    torch.cuda.empty_cache()
+    op = NA_operator(m, device=dev.index)
     torch.cuda.synchronize()
     out["symmetrised_build_s"] = round(time.time() - t, 1)
     out["symmetrised_nnz"] = int(m.get_nnz())
-    net = ws.warm_start_net.load(os.path.join(ROOT, "flashx_b200", "warmstart_weights.f32"))
+    net = ws.warm_start_net.load(os.path.join(ROOT, "flashx_b200", "warmstart_weights.f32"), dev.index)
     for name, prec, learned in (("plain", "plain", False), ("mixed", "mixed", False),
                                 ("mixed_learned", "mixed", True)):
         o = ws.eigen_opts(16, 1e-6, prec)
         ms, r = _timed_solve(torch, dev, lambda: compute_eigen(
-            op, True, o, X0=net.start_block(op, 0, o.block_size) if learned else None), reps=2)
+            op, True, o, X0=net.start_block(op, 0, o.block_size) if learned else None), reps=1)
         out[name] = _solve_summary(ms, r)
         out[name]["block"] = o.block_size
         if learned:
             out[name]["spmm_calls"] += ws.SPMM_PER_START
+    out["speedup_mixed_vs_plain"] = round(out["plain"]["ms"] / out["mixed"]["ms"], 3)
+    out["speedup_learned_mixed_vs_plain"] = round(out["plain"]["ms"] / out["mixed_learned"]["ms"], 3)
+    del op, m
+    torch.cuda.empty_cache()
     return out
 
 
@@ -652,9 +759,17 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if a.impl == "reference":
         return run_reference(a, rank, world)
+    if a.dense_only:
+        if rank == 0:
+            import torch
+            peak, _ = read_peaks()
+            print(json.dumps(dense_measure(torch.device("cuda", local), peak)), flush=True)
+        return
     if a.large:
         if rank == 0:
-            print(json.dumps(large_run(a)), flush=True)
+            import torch
+            peak, _ = read_peaks()
+            print(json.dumps(large_measure(a, torch.device("cuda", local), peak)), flush=True)
         return
 
     import torch
@@ -768,12 +883,21 @@ def main():
                "sample": cpu_sample_desc(a, brows, nnz_s, nnz, nb, nthreads, model) + f"; median of {reps}",
                "cpu_config": cpu_config_s16(nthreads)}
 
-    eig = prk = None
+    sweep = dense = None
+    if rank == 0 and not a.skip_sweep:
+        sweep = sweep_measure(a, m, n_rows, nnz, dev, peak)
+    if rank == 0 and not a.skip_dense:
+        dense = dense_measure(dev, peak)
+
+    eig = prk = large = None
     if rank == 0 and not a.skip_eigen:
         del m, X, Y
         torch.cuda.empty_cache()
         eig = eigen_measure(a, dev)
         prk = pagerank_measure(a, dev)
+    if rank == 0 and not a.skip_large:
+        torch.cuda.empty_cache()
+        large = large_measure(a, dev, peak)
 
     if rank == 0:
         line = {
@@ -793,15 +917,18 @@ def main():
                                     "scratch_bytes": scratch_bytes}},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
-                         "kernel": "pack_hot_kernel + spmm_kernel + spmm_fixup_kernel, per fmx_spmm call",
+                         "kernel": "pack_hot_kernel + spmm_wide_kernel + spmm_fixup kernels, per fmx_spmm call",
                          "traffic": traffic},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": a.steps * kernels,
             "clocks": clk,
+            "sweep": sweep,
+            "dense": dense,
             "eigen": eig,
             "pagerank": prk,
             "streamed": streamed,
+            "large": large,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

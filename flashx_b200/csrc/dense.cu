@@ -1106,20 +1106,28 @@ __global__ void chol_inv_kernel(const double *__restrict__ G, int b, double *__r
 }
 
 // Symmetric eigendecomposition H = V diag(w) V^T by cyclic Jacobi rotations
-// (round-robin pairs, b/2 rotations in parallel per step).  Eigenvalues in
-// descending order, V columns matching.  One CTA of 32 threads.
-__global__ void jacobi_eig_kernel(const double *__restrict__ H, int b, double *__restrict__ w, double *__restrict__ V,
-		int max_sweeps)
+// (round-robin pairs: m/2 disjoint rotations per step).  Eigenvalues in
+// descending order, V columns matching.  One CTA of kJacobiThreads threads:
+// a step's row and column updates are (pair, index) items spread over the
+// threads (disjoint pairs touch disjoint rows and columns), the off-diagonal
+// norm is a CTA reduction, and the final order is a parallel rank count.
+constexpr int kJacobiThreads = 256;
+
+__global__ void __launch_bounds__(kJacobiThreads) jacobi_eig_kernel(const double *__restrict__ H, int b,
+		double *__restrict__ w, double *__restrict__ V, int max_sweeps)
 {
 	extern __shared__ double dyn[];                  // two 64 x 65 FP64 matrices
 	double (*A)[65] = reinterpret_cast<double (*)[65]>(dyn);
 	double (*Q)[65] = reinterpret_cast<double (*)[65]>(dyn + 64 * 65);
 	__shared__ int pr[32], pc[32];
 	__shared__ double cs[32], sn[32];
-	__shared__ int order[64];
+	__shared__ int cand[64], order[64];
+	__shared__ int ncand;
+	__shared__ double red_o[kJacobiThreads / 32], red_d[kJacobiThreads / 32];
 	__shared__ double off;
-	const int t = threadIdx.x;
+	const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
 	const int m = (b + 1) & ~1;                       // even size (pad with a zero row/column)
+	const int half = m / 2;
 	for (int i = t; i < m * m; i += blockDim.x) {
 		const int r = i / m, c = i % m;
 		A[r][c] = (r < b && c < b) ? 0.5 * (H[r * b + c] + H[c * b + r]) : 0.0;
@@ -1127,67 +1135,84 @@ __global__ void jacobi_eig_kernel(const double *__restrict__ H, int b, double *_
 	}
 	__syncthreads();
 	for (int sweep = 0; sweep < max_sweeps; sweep++) {
+		double so = 0, sd = 0;
+		for (int i = t; i < m * m; i += blockDim.x) {
+			const int r = i / m, c = i % m;
+			const double v = A[r][c] * A[r][c];
+			if (r == c) sd += v; else so += v;
+		}
+		for (int o = 16; o > 0; o >>= 1) {
+			so += __shfl_xor_sync(0xffffffffu, so, o);
+			sd += __shfl_xor_sync(0xffffffffu, sd, o);
+		}
+		if (lane == 0) { red_o[wid] = so; red_d[wid] = sd; }
+		__syncthreads();
 		if (t == 0) {
-			double s = 0, d = 0;
-			for (int r = 0; r < m; r++)
-				for (int c = 0; c < m; c++) (r == c ? d : s) += A[r][c] * A[r][c];
-			off = s / (d > 0 ? d : 1.0);
+			double a = 0, d = 0;
+			for (int i = 0; i < int(blockDim.x) / 32; i++) { a += red_o[i]; d += red_d[i]; }
+			off = a / (d > 0 ? d : 1.0);
 		}
 		__syncthreads();
 		if (off < 1e-30) break;
 		for (int step = 0; step < m - 1; step++) {
 			// round-robin tournament pairing of 0..m-1
-			if (t < m / 2) {
+			if (t < half) {
 				int a = t == 0 ? 0 : 1 + (t - 1 + step) % (m - 1);
 				int bb = 1 + (m - 2 - t + step) % (m - 1);
 				if (a > bb) { int x = a; a = bb; bb = x; }
 				pr[t] = a; pc[t] = bb;
 				const double app = A[a][a], aqq = A[bb][bb], apq = A[a][bb];
-				double c = 1, s = 0;
+				double c = 1, s2 = 0;
 				if (fabs(apq) > 1e-300) {
 					const double tau = (aqq - app) / (2 * apq);
 					const double tt = (tau >= 0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1 + tau * tau));
 					c = 1 / sqrt(1 + tt * tt);
-					s = tt * c;
+					s2 = tt * c;
 				}
-				cs[t] = c; sn[t] = s;
+				cs[t] = c; sn[t] = s2;
 			}
 			__syncthreads();
 			// rows: A <- J^T A
-			for (int k = t; k < m; k += blockDim.x)
-				for (int q = 0; q < m / 2; q++) {
-					const int p0 = pr[q], p1 = pc[q];
-					const double x = A[p0][k], y = A[p1][k];
-					A[p0][k] = cs[q] * x - sn[q] * y;
-					A[p1][k] = sn[q] * x + cs[q] * y;
-				}
+			for (int i = t; i < half * m; i += blockDim.x) {
+				const int q = i / m, k = i % m;
+				const int p0 = pr[q], p1 = pc[q];
+				const double x = A[p0][k], y = A[p1][k];
+				A[p0][k] = cs[q] * x - sn[q] * y;
+				A[p1][k] = sn[q] * x + cs[q] * y;
+			}
 			__syncthreads();
 			// columns: A <- A J, Q <- Q J
-			for (int k = t; k < m; k += blockDim.x)
-				for (int q = 0; q < m / 2; q++) {
-					const int p0 = pr[q], p1 = pc[q];
-					double x = A[k][p0], y = A[k][p1];
-					A[k][p0] = cs[q] * x - sn[q] * y;
-					A[k][p1] = sn[q] * x + cs[q] * y;
-					x = Q[k][p0]; y = Q[k][p1];
-					Q[k][p0] = cs[q] * x - sn[q] * y;
-					Q[k][p1] = sn[q] * x + cs[q] * y;
-				}
+			for (int i = t; i < half * m; i += blockDim.x) {
+				const int q = i / m, k = i % m;
+				const int p0 = pr[q], p1 = pc[q];
+				double x = A[k][p0], y = A[k][p1];
+				A[k][p0] = cs[q] * x - sn[q] * y;
+				A[k][p1] = sn[q] * x + cs[q] * y;
+				x = Q[k][p0]; y = Q[k][p1];
+				Q[k][p0] = cs[q] * x - sn[q] * y;
+				Q[k][p1] = sn[q] * x + cs[q] * y;
+			}
 			__syncthreads();
 		}
 	}
+	// descending order of the b real eigenvalues (the padding one, if any, is dropped)
 	if (t == 0) {
-		// descending order of the b real eigenvalues (the padding one, if any, is dropped)
-		int idx[64];
 		int cnt = 0;
 		for (int i = 0; i < m; i++) {
-			bool pad = (m != b) && (fabs(Q[b][i]) > 0.5);   // eigenvector of the zero padding
-			if (!pad && cnt < b) idx[cnt++] = i;
+			const bool pad = (m != b) && (fabs(Q[b][i]) > 0.5);   // eigenvector of the zero padding
+			if (!pad && cnt < b) cand[cnt++] = i;
 		}
-		for (int i = 0; i < cnt; i++)
-			for (int j = i + 1; j < cnt; j++)
-				if (A[idx[j]][idx[j]] > A[idx[i]][idx[i]]) { int x = idx[i]; idx[i] = idx[j]; idx[j] = x; }
-		for (int i = 0; i < cnt; i++) order[i] = idx[i];
+		ncand = cnt;
+	}
+	__syncthreads();
+	if (t < ncand) {
+		const double mine = A[cand[t]][cand[t]];
+		int rank = 0;
+		for (int j = 0; j < ncand; j++) {
+			const double o = A[cand[j]][cand[j]];
+			rank += (o > mine) || (o == mine && j < t);
+		}
+		order[rank] = cand[t];
 	}
 	__syncthreads();
 	for (int i = t; i < b; i += blockDim.x) w[i] = A[order[i]][order[i]];
@@ -1344,7 +1369,7 @@ int fmx_dense_sym_eig(const double *H, int b, double *w, double *V, void *stream
 	if (b < 1 || b > 64) return set_error(FMX_ERR_UNSUPPORTED, "b in 1..64");
 	const int smem = 2 * 64 * 65 * int(sizeof(double));
 	DCUDA_TRY(cudaFuncSetAttribute(jacobi_eig_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-	jacobi_eig_kernel<<<1, 32, smem, static_cast<cudaStream_t>(stream)>>>(H, b, w, V, 30);
+	jacobi_eig_kernel<<<1, kJacobiThreads, smem, static_cast<cudaStream_t>(stream)>>>(H, b, w, V, 30);
 	DCUDA_TRY(cudaGetLastError());
 	return FMX_OK;
 }
