@@ -95,6 +95,7 @@ _SIGS = {
     "fmx_spmm_noalloc": (_int, [_vp, _vp, _i64, _vp, _i64, _i64, _vp]),
     "fmx_matrix_schedule": (_int, [_vp, _P(_u64), _P(_u64), _P(_u64), _P(_u64)]),
     "fmx_matrix_hot": (_int, [_vp, _P(_u64), _P(_u64), _P(_u64)]),
+    "fmx_matrix_layout_digest": (_int, [_vp, _int, _P(_u64)]),
     "fmx_dense_gemm": (_int, [_int, _vp, _i64, _i64, _int, _vp, _int, _int, _vp, _i64, _vp, _vp]),
     "fmx_dense_gram_parts": (_int, [_int, _i64]),
     "fmx_dense_gram": (_int, [_int, _vp, _i64, _int, _vp, _i64, _int, _i64, _vp, _vp, _vp, _vp]),

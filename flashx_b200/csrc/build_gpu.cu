@@ -11,7 +11,7 @@
 //   3. first-of-run flags (all ones without dedup), exclusive scan, scatter
 //   4. row pointers from the row boundaries of the sorted keys
 //   5. values gathered by the sorted input positions
-#include "fmx_internal.h"
+#include "part.h"
 
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
@@ -23,7 +23,7 @@
 namespace fmx {
 namespace gbuild {
 
-constexpr int kThreads = 256;
+constexpr int kBuildThreads = 256;
 
 #define BCUDA_TRY(call)                                                         \
 	do {                                                                        \
@@ -38,7 +38,7 @@ unsigned grid_for(uint64_t n)
 	int dev = 0, sms = 0;
 	cudaGetDevice(&dev);
 	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-	return unsigned(std::max<uint64_t>(1, std::min<uint64_t>((n + kThreads - 1) / kThreads, uint64_t(std::max(sms, 1)) * 16)));
+	return unsigned(std::max<uint64_t>(1, std::min<uint64_t>((n + kBuildThreads - 1) / kBuildThreads, uint64_t(std::max(sms, 1)) * 16)));
 }
 
 // largest vertex id over both endpoints (for nrows / ncols = 0: the
@@ -129,8 +129,13 @@ struct dbuf {
 
 } // namespace gbuild
 
-int edges_to_csr_device(const uint32_t *src, const uint32_t *dst, const void *vals, int val_type, uint64_t nedges,
-		uint64_t nrows, uint64_t ncols, int flags, cudaStream_t st, host_csr &out)
+dev_csr::~dev_csr()
+{
+	for (void *q : own) cudaFreeAsync(q, st);
+}
+
+int edges_to_dev_csr(const uint32_t *src, const uint32_t *dst, const void *vals, int val_type, uint64_t nedges,
+		uint64_t nrows, uint64_t ncols, int flags, cudaStream_t st, dev_csr &out)
 {
 	using namespace gbuild;
 	if (nedges >= (1ull << 31)) return set_error(FMX_ERR_UNSUPPORTED, "the device builder takes < 2^31 edges");
@@ -142,7 +147,7 @@ int edges_to_csr_device(const uint32_t *src, const uint32_t *dst, const void *va
 		unsigned int h = 0;
 		if (int rc = b.get(&mx, 1)) return rc;
 		BCUDA_TRY(cudaMemsetAsync(mx, 0, sizeof(unsigned int), st));
-		if (nedges) max_ids_kernel<<<grid_for(nedges), kThreads, 0, st>>>(src, dst, nedges, mx);
+		if (nedges) max_ids_kernel<<<grid_for(nedges), kBuildThreads, 0, st>>>(src, dst, nedges, mx);
 		BCUDA_TRY(cudaGetLastError());
 		BCUDA_TRY(cudaMemcpyAsync(&h, mx, sizeof(h), cudaMemcpyDeviceToHost, st));
 		BCUDA_TRY(cudaStreamSynchronize(st));
@@ -160,13 +165,12 @@ int edges_to_csr_device(const uint32_t *src, const uint32_t *dst, const void *va
 	uint64_t *k0, *k1;
 	uint32_t *p0, *p1, *flag, *at, *row;
 	unsigned long long *bad;
-	int32_t *col;
-	uint32_t *opos, *row_ptr;
+	uint32_t *opos;
 	for (int rc : {b.get(&k0, nedges), b.get(&k1, nedges), b.get(&p0, nedges), b.get(&p1, nedges),
 			b.get(&flag, nedges + 1), b.get(&at, nedges + 1), b.get(&bad, 1)})
 		if (rc) return rc;
 	BCUDA_TRY(cudaMemsetAsync(bad, 0, sizeof(unsigned long long), st));
-	if (nedges) keys_kernel<<<grid_for(nedges), kThreads, 0, st>>>(src, dst, nedges, (flags & FMX_BUILD_KEEP_SELF_LOOPS) ? 1 : 0,
+	if (nedges) keys_kernel<<<grid_for(nedges), kBuildThreads, 0, st>>>(src, dst, nedges, (flags & FMX_BUILD_KEEP_SELF_LOOPS) ? 1 : 0,
 			cbits, nrows, ncols, k0, p0, bad);
 	BCUDA_TRY(cudaGetLastError());
 	// stable sort over the key bits in use plus one: kept keys are below
@@ -181,7 +185,7 @@ int edges_to_csr_device(const uint32_t *src, const uint32_t *dst, const void *va
 	BCUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp, tbytes, dk, dp, n, 0, end_bit, st));
 	const uint64_t *keys = dk.Current();
 	const uint32_t *pos = dp.Current();
-	if (nedges) flags_kernel<<<grid_for(nedges), kThreads, 0, st>>>(keys, nedges, (flags & FMX_BUILD_DEDUP) ? 1 : 0, flag);
+	if (nedges) flags_kernel<<<grid_for(nedges), kBuildThreads, 0, st>>>(keys, nedges, (flags & FMX_BUILD_DEDUP) ? 1 : 0, flag);
 	BCUDA_TRY(cudaGetLastError());
 	BCUDA_TRY(cudaMemsetAsync(flag + nedges, 0, sizeof(uint32_t), st));
 	size_t sbytes = 0;
@@ -196,31 +200,39 @@ int edges_to_csr_device(const uint32_t *src, const uint32_t *dst, const void *va
 	BCUDA_TRY(cudaStreamSynchronize(st));
 	if (hbad) return set_error(FMX_ERR_INVAL, "%llu edges have ids outside %llu x %llu", hbad,
 			(unsigned long long)nrows, (unsigned long long)ncols);
-	for (int rc : {b.get(&col, nnz), b.get(&opos, nnz), b.get(&row, nnz), b.get(&row_ptr, nrows + 1)})
+	// the CSR arrays outlive this call: they belong to `out`
+	out.st = st;
+	auto keep = [&](void **q, size_t bytes) -> int {
+		cudaError_t e = work_alloc(q, std::max<size_t>(bytes, 16), st);
+		if (e != cudaSuccess) return set_error(FMX_ERR_OOM, "device builder: %zu bytes: %s", bytes, cudaGetErrorString(e));
+		out.own.push_back(*q);
+		return FMX_OK;
+	};
+	int32_t *col = nullptr;
+	uint32_t *row_ptr = nullptr;
+	char *gv = nullptr;
+	for (int rc : {keep(reinterpret_cast<void **>(&col), size_t(nnz) * sizeof(int32_t)),
+			keep(reinterpret_cast<void **>(&row_ptr), (nrows + 1) * sizeof(uint32_t)), b.get(&opos, nnz),
+			b.get(&row, nnz)})
 		if (rc) return rc;
-	if (nedges) scatter_kernel<<<grid_for(nedges), kThreads, 0, st>>>(keys, pos, flag, at, nedges, (1ull << cbits) - 1,
+	if (nedges) scatter_kernel<<<grid_for(nedges), kBuildThreads, 0, st>>>(keys, pos, flag, at, nedges, (1ull << cbits) - 1,
 			col, opos, row);
 	BCUDA_TRY(cudaGetLastError());
-	rowptr_kernel<<<grid_for(uint64_t(nnz) + 1), kThreads, 0, st>>>(row, nnz, nrows, row_ptr);
+	rowptr_kernel<<<grid_for(uint64_t(nnz) + 1), kBuildThreads, 0, st>>>(row, nnz, nrows, row_ptr);
 	BCUDA_TRY(cudaGetLastError());
+	if (esize) {
+		if (int rc = keep(reinterpret_cast<void **>(&gv), size_t(nnz) * esize)) return rc;
+		if (nnz) gather_kernel<<<grid_for(nnz), kBuildThreads, 0, st>>>(static_cast<const char *>(vals), esize, opos, nnz, gv);
+		BCUDA_TRY(cudaGetLastError());
+	}
 	out.nrows = nrows;
 	out.ncols = ncols;
 	out.nnz = nnz;
 	out.prim = val_type;
 	out.esize = esize;
-	out.row_ptr.resize(nrows + 1);
-	out.col.resize(nnz);
-	out.val.resize(size_t(nnz) * esize);
-	BCUDA_TRY(cudaMemcpyAsync(out.row_ptr.data(), row_ptr, (nrows + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-	if (nnz) BCUDA_TRY(cudaMemcpyAsync(out.col.data(), col, size_t(nnz) * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
-	if (esize && nnz) {
-		char *gv = nullptr;
-		if (int rc = b.get(&gv, size_t(nnz) * esize)) return rc;
-		gather_kernel<<<grid_for(nnz), kThreads, 0, st>>>(static_cast<const char *>(vals), esize, opos, nnz, gv);
-		BCUDA_TRY(cudaGetLastError());
-		BCUDA_TRY(cudaMemcpyAsync(out.val.data(), gv, size_t(nnz) * esize, cudaMemcpyDeviceToHost, st));
-	}
-	BCUDA_TRY(cudaStreamSynchronize(st));
+	out.row_ptr = row_ptr;
+	out.col = col;
+	out.val = gv;
 	return FMX_OK;
 }
 

@@ -86,12 +86,6 @@ struct host_csr {
 };
 int decode_to_csr(const image &img, host_csr &out, int nthreads);
 
-// The same CSR from a device-resident edge list (sorted and deduplicated on
-// the GPU of the current device, then copied to the host); flags as
-// fmx_image_build's.
-int edges_to_csr_device(const uint32_t *src, const uint32_t *dst, const void *vals, int val_type, uint64_t nedges,
-		uint64_t nrows, uint64_t ncols, int flags, cudaStream_t st, host_csr &out);
-
 int default_threads();
 
 // Stream-ordered workspace from the current device's library pool (freed

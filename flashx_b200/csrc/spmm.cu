@@ -62,119 +62,7 @@
 #include <mutex>
 #include <thread>
 
-namespace fmx {
-
-// ---------------------------------------------------------------------------
-// Schedule parameters
-// ---------------------------------------------------------------------------
-constexpr uint32_t kExactMax = FMX_EXACT_ROW_MAX;  // rows summed by one lane group
-constexpr uint32_t kChunk = 256;        // most entries per chunk of a longer row
-constexpr uint32_t kRange = 256;        // target entries per multi-row range
-constexpr uint32_t kLongChunks = 8;     // heavy rows with more chunks get a warp each in the fixup
-#ifndef FMX_HOT_MAX
-#define FMX_HOT_MAX (1u << 20)
-#endif
-constexpr uint32_t kHotMax = FMX_HOT_MAX;  // most packed hot columns
-constexpr int kPanelBytes = 128;        // X row bytes per panel (hot pack row)
-constexpr int kPartialStride = 256;     // AccT slots per partial (one panel)
-constexpr int kThreads = 256;           // threads per SpMM block
-#ifndef FMX_SPMM_MIN_BLOCKS
-#define FMX_SPMM_MIN_BLOCKS 5           // resident blocks per SM the register budget targets
-#endif
-#ifndef FMX_SPMM_MIN_BLOCKS_2B
-#define FMX_SPMM_MIN_BLOCKS_2B 4        // the same for 2-byte (BF16) operands: measured at R-MAT
-                                        // scale 22, k = 16, 4 blocks of more registers beat 5
-                                        // (0.837 against 0.894 ms), while FP32 at scale 24
-                                        // prefers 5 (2.56 against 2.73 ms)
-#endif
-constexpr int kStep = 8;                // entries per index load group (alignment unit)
-constexpr uint32_t kEnd = 0x80000000u;  // last entry of a row
-constexpr uint32_t kHot = 0x40000000u;  // entry refers to a hot slot
-constexpr uint32_t kIdxMask = 0x3FFFFFFFu;
-constexpr uint32_t kNoSlot = 0xFFFFFFFFu;
-
-struct range_t {
-	uint32_t e0;         // first entry (a multiple of kStep)
-	uint32_t len;        // entries, padded to a multiple of kStep
-	uint32_t row0;       // first row (row runs)
-	uint32_t slot;       // kNoSlot for row runs; else the chunk's partial slot
-};
-struct heavy_row {
-	int32_t row;
-	uint32_t first, count;
-};
-
-#define CUDA_TRY(call)                                                          \
-	do {                                                                        \
-		cudaError_t err__ = (call);                                             \
-		if (err__ != cudaSuccess)                                               \
-			return set_error(FMX_ERR_CUDA, "%s failed: %s (%s:%d)", #call,      \
-					cudaGetErrorString(err__), __FILE__, __LINE__);             \
-	} while (0)
-
-// Device-resident part of one orientation of a matrix.
-struct gpu_part {
-	int device = 0;
-	uint64_t nrows = 0, ncols = 0, nnz = 0;
-	int prim = 0;
-	size_t esize = 0;
-	uint32_t *col = nullptr;
-	void *val = nullptr;
-	int32_t *hot_col = nullptr;
-	uint32_t n_hot = 0;
-	void *xhot = nullptr;                // (n_hot + 1) * kPanelBytes
-	uint32_t n_exact = 0;                // rows summed in the reference's order
-	range_t *ranges = nullptr;
-	uint32_t n_ranges = 0;
-	heavy_row *heavy = nullptr;
-	uint32_t n_heavy = 0;
-	uint32_t n_long_heavy = 0;           // the first heavy rows, of more than kLongChunks chunks
-	uint32_t n_block_heavy = 0;          // the first of those, of more than kBlockChunks chunks
-	uint32_t n_partials = 0;
-	void *partial = nullptr;
-	uint64_t hot_entries = 0;            // entries that read the hot pack
-	uint64_t bytes = 0;
-	// streamed part: the entry stream stays in pinned host memory and each
-	// SpMM copies it slice by slice into two device slots (copy_st), the
-	// kernel of one slice overlapping the copy of the next
-	struct slice_t { uint64_t e0, e1; uint32_t r0, nr; };   // entries [e0, e1), ranges [r0, r0 + nr)
-	bool streamed = false;
-	uint32_t *h_col = nullptr;
-	void *h_val = nullptr;
-	std::vector<slice_t> slices;
-	uint32_t *slot_col[2] = {nullptr, nullptr};
-	void *slot_val[2] = {nullptr, nullptr};
-	cudaStream_t copy_st = nullptr;
-	cudaEvent_t ev_start = nullptr, ev_copied[2] = {nullptr, nullptr}, ev_free[2] = {nullptr, nullptr};
-	uint64_t host_bytes = 0;
-	// staging buffers of fmx_spmm_host (grow-only, guarded by stage_mu)
-	std::mutex stage_mu;
-	void *stage_x = nullptr, *stage_y = nullptr;
-	size_t stage_xb = 0, stage_yb = 0;
-	~gpu_part() {
-		int cur = 0;
-		cudaGetDevice(&cur);
-		cudaSetDevice(device);
-		void *ps[] = {col, val, hot_col, xhot, ranges, heavy, partial, stage_x, stage_y, slot_col[0], slot_col[1],
-				slot_val[0], slot_val[1]};
-		for (void *p : ps)
-			if (p) cudaFree(p);
-		if (h_col) cudaFreeHost(h_col);
-		if (h_val) cudaFreeHost(h_val);
-		for (cudaEvent_t e : {ev_start, ev_copied[0], ev_copied[1], ev_free[0], ev_free[1]})
-			if (e) cudaEventDestroy(e);
-		if (copy_st) cudaStreamDestroy(copy_st);
-		cudaSetDevice(cur);
-	}
-};
-
-} // namespace fmx
-
-struct fmx_matrix {
-	std::shared_ptr<fmx::gpu_part> a;    // this orientation
-	std::shared_ptr<fmx::gpu_part> at;   // the transpose (null when symmetric)
-	bool symmetric = true;
-};
+#include "part.h"
 
 namespace fmx {
 
@@ -446,11 +334,6 @@ __device__ __forceinline__ void store_row(const spmm_args &a, int32_t row, int c
 template <int U>
 __device__ __forceinline__ void ld_idx(const uint32_t *col, uint32_t step, uint32_t (&r)[U])
 {
-	if constexpr (U == 2) {
-		const uint2 a = __ldg(reinterpret_cast<const uint2 *>(col) + step);
-		r[0] = a.x; r[1] = a.y;
-		return;
-	}
 	const uint4 *p = reinterpret_cast<const uint4 *>(col) + (U / 4) * step;
 #pragma unroll
 	for (int q = 0; q < U / 4; q++) {
@@ -467,20 +350,17 @@ __device__ __forceinline__ void ld_w(const void *val, uint32_t step, A (&w)[U])
 #pragma unroll
 		for (int u = 0; u < U; u++) w[u] = A(1);
 	} else {
-		if constexpr (U * sizeof(WT) == 8) {
-			// two 4-byte weights (a step of 2 entries)
-			const uint2 b = __ldcs(reinterpret_cast<const uint2 *>(static_cast<const WT *>(val) + size_t(step) * U));
-			WT t[2];
-			memcpy(t, &b, 8);
-			w[0] = A(t[0]);
-			w[1] = A(t[1]);
-		} else {
+		{
+			// cached like the column ids: the streaming form, which skips
+			// L1, fetched each weight line from L2 again at every step (in
+			// the 32-byte-lane kernel, cached 32-byte weight loads took a
+			// weighted call at R-MAT scale 24, k = 16 from 3.43 to 2.58 ms)
 			const uint4 *p = reinterpret_cast<const uint4 *>(static_cast<const WT *>(val) + size_t(step) * U);
 			constexpr int per = int(16 / sizeof(WT));
 			static_assert(U % per == 0, "whole 16-byte weight loads");
 #pragma unroll
 			for (int q = 0; q < U / per; q++) {
-				uint4 a = __ldcs(p + q);
+				uint4 a = __ldg(p + q);
 				WT t[per];
 				memcpy(t, &a, 16);
 #pragma unroll
@@ -645,9 +525,6 @@ spmm_kernel(const spmm_args a, const pr_epi e)
 #ifndef FMX_WIDE_MIN_BLOCKS
 #define FMX_WIDE_MIN_BLOCKS 4
 #endif
-#ifndef FMX_WIDE_STEP
-#define FMX_WIDE_STEP 4
-#endif
 
 __device__ __forceinline__ void ld32_nc(const void *p, uint32_t (&r)[8])
 {
@@ -695,25 +572,38 @@ __device__ __forceinline__ void run_range_wide(const spmm_args &a, const range_t
 #pragma unroll
 	for (int i = 0; i < VEC / 2; i++) p[i] = 0;
 	uint32_t row = rg.row0;
-	uint32_t s = rg.e0 / U;
-	const uint32_t s_end = s + rg.len / U;
-	uint32_t raw[U];
-	ld_idx<U>(a.col, s, raw);
+	// pairs of 4-entry steps (a range is a whole number of kStep = 8
+	// entries): one 32-byte load of 8 column ids, and of 8 weights, per lane
+	// per pair, issued with the first step's gathers; the next pair's column
+	// ids load with the second step's gathers
+	static_assert(U == 4 && kStep == 2 * U, "pairs of 4-entry steps");
+	uint32_t s = rg.e0 / kStep;
+	const uint32_t s_end = s + rg.len / kStep;
+	uint32_t raw8[2 * U];
+	ld32_nc(a.col + size_t(s) * kStep, raw8);
 	for (; s < s_end; s++) {
+		uint32_t w8[2 * U];
+		if constexpr (!kBinary) ld32_nc(static_cast<const WT *>(a.val) + size_t(s) * kStep, w8);
+#pragma unroll
+		for (int half = 0; half < 2; half++) {
 		float w[U];
-		if constexpr (!kBinary) ld_w<WT, float, U>(a.val, s, w);
+		if constexpr (!kBinary) {
+#pragma unroll
+			for (int u = 0; u < U; u++) w[u] = __uint_as_float(w8[half * U + u]);
+		}
 		uint32_t xv[U][8];
 		float sc[U];
 		uint32_t ends = 0;
 #pragma unroll
 		for (int u = 0; u < U; u++) {
-			const uint32_t c = raw[u] & kIdxMask;
-			const bool hot = raw[u] & kHot;
+			const uint32_t rw = raw8[half * U + u];
+			const uint32_t c = rw & kIdxMask;
+			const bool hot = rw & kHot;
 			ld32_nc((hot ? Hb : Xb) + uint64_t(c) * (hot ? hs : xs), xv[u]);
 			if constexpr (SCALE_IN) sc[u] = hot ? 1.f : static_cast<const float *>(a.s_in)[c];
-			ends |= (raw[u] >> 31) << u;
+			ends |= (rw >> 31) << u;
 		}
-		if (s + 1 < s_end) ld_idx<U>(a.col, s + 1, raw);
+		if (half == 1 && s + 1 < s_end) ld32_nc(a.col + size_t(s + 1) * kStep, raw8);
 #pragma unroll
 		for (int u = 0; u < U; u++) {
 			float f[VEC];
@@ -756,6 +646,7 @@ __device__ __forceinline__ void run_range_wide(const spmm_args &a, const range_t
 #pragma unroll
 			for (int i = 0; i < VEC / 2; i++) p[i] = end ? 0ull : p[i];
 			row += end;
+		}
 		}
 	}
 	if (!runs) {
@@ -946,7 +837,6 @@ __device__ __forceinline__ void chunk_sums(const A *pc, uint32_t part, uint32_t 
 // combined by the xor tree and the 8 warp sums added in warp order.  The
 // chain of one part is then at most count / (8 * 32 / L) chunks long instead
 // of count / (32 / L), which bounded the whole fixup by its longest row.
-constexpr uint32_t kBlockChunks = 64;
 template <class YT, class A, bool SCALE_OUT, bool EPI = false>
 __global__ void __launch_bounds__(256) spmm_fixup_block_kernel(const heavy_row *heavy, const A *partial, YT *Y,
 		int64_t ldy, int k, const A *s_out, int L, const pr_epi e)
@@ -1206,7 +1096,8 @@ static int make_part(const host_csr &csr, int device, std::shared_ptr<gpu_part> 
 
 	// Work segments: runs of consecutive rows (every row in order; an exact
 	// row with its entries, an empty or longer row as one zero-row entry),
-	// then the equal chunks of the longer rows.  Each segment starts at a
+	// then the equal chunks of the longer rows (the rule of seg_row_len in
+	// part.h, which make_part_device follows too).  Each segment starts at a
 	// multiple of kStep in the stream and is padded to one.
 	const uint32_t zero_entry = 0u | kHot;          // slot 0: the zero row
 	struct seg_t { uint64_t row0, row1; uint32_t b, e; uint32_t slot; uint64_t at; uint32_t len; };
@@ -1214,18 +1105,18 @@ static int make_part(const host_csr &csr, int device, std::shared_ptr<gpu_part> 
 	std::vector<heavy_row> heavy;
 	uint32_t n_exact = 0;
 	{
-		uint64_t run = 0;                        // real entries in the open run
+		uint64_t L = 0, bucket = ~0ull;           // lens of the rows before r
 		for (uint64_t r = 0; r < n; r++) {
 			const uint32_t d = csr.row_ptr[r + 1] - csr.row_ptr[r];
-			const uint32_t len = (d >= 1 && d <= kExactMax) ? d : 1;
+			const uint32_t len = seg_row_len(d);
 			n_exact += (d >= 1 && d <= kExactMax);
-			if (segs.empty() || run >= kRange) {
+			if (L / kRange != bucket) {
 				segs.push_back({r, r + 1, 0, 0, kNoSlot, 0, 0});
-				run = 0;
+				bucket = L / kRange;
 			} else {
 				segs.back().row1 = r + 1;
 			}
-			run += len;
+			L += len;
 			segs.back().len += len;
 		}
 	}
@@ -1441,8 +1332,7 @@ static int launch_one(const gpu_part &p, const spmm_args &a, cudaStream_t st)
 template <class XT, class YT, class WT, bool SI, bool SO>
 static int launch_wide(const gpu_part &p, const spmm_args &a, cudaStream_t st)
 {
-	// BF16 lanes hold 16 elements: a step of 2 entries keeps them in registers
-	auto kern = spmm_wide_kernel<XT, YT, WT, sizeof(XT) == 2 ? 2 : FMX_WIDE_STEP, SI, SO>;
+	auto kern = spmm_wide_kernel<XT, YT, WT, 4, SI, SO>;
 	static std::atomic<unsigned> blocks[64];
 	const unsigned b = cached_blocks(blocks[p.device & 63], kern, p.device);
 	kern<<<b, kThreads, 0, st>>>(a);
@@ -1463,7 +1353,8 @@ static int launch_t(const gpu_part &p, spmm_args a, bool sin, bool sout, cudaStr
 		CUDA_TRY(cudaGetLastError());
 	}
 	int rc = over_slices(p, a, st, [&](const spmm_args &sa) -> int {
-		if constexpr (std::is_same<A, float>::value && (std::is_same<WT, void>::value || std::is_same<WT, float>::value)) {
+		if constexpr (std::is_same<A, float>::value && sizeof(XT) == 4 &&
+				(std::is_same<WT, void>::value || std::is_same<WT, float>::value)) {
 			if (wide) {
 				if (sin && sout) return launch_wide<XT, YT, WT, true, true>(p, sa, st);
 				if (sin) return launch_wide<XT, YT, WT, true, false>(p, sa, st);
@@ -1883,14 +1774,20 @@ int fmx_matrix_build_device(const uint32_t *src, const uint32_t *dst, const void
 	int rc = m ? FMX_OK : set_error(FMX_ERR_OOM, "out of host memory");
 	cudaStream_t st = static_cast<cudaStream_t>(stream);
 	try {
-		host_csr csr;
-		if (!rc) rc = edges_to_csr_device(src, dst, vals, val_type, nedges, nrows, ncols, flags, st, csr);
-		if (!rc) rc = make_part(csr, device, m->a);
-		if (!rc && (flags & FMX_BUILD_TRANSPOSE)) {
-			host_csr t;
-			rc = edges_to_csr_device(dst, src, vals, val_type, nedges, csr.ncols, csr.nrows, flags, st, t);
-			if (!rc) rc = make_part(t, device, m->at);
+		uint64_t nr = nrows, nc = ncols;
+		{
+			dev_csr csr;
+			if (!rc) rc = edges_to_dev_csr(src, dst, vals, val_type, nedges, nrows, ncols, flags, st, csr);
+			if (!rc) rc = make_part_device(csr, device, st, m->a);
+			nr = csr.nrows;
+			nc = csr.ncols;
 		}
+		if (!rc && (flags & FMX_BUILD_TRANSPOSE)) {
+			dev_csr t;
+			rc = edges_to_dev_csr(dst, src, vals, val_type, nedges, nc, nr, flags, st, t);
+			if (!rc) rc = make_part_device(t, device, st, m->at);
+		}
+		if (!rc && cudaStreamSynchronize(st) != cudaSuccess) rc = set_error(FMX_ERR_CUDA, "device builder failed");
 	} catch (const std::bad_alloc &) {
 		rc = set_error(FMX_ERR_OOM, "host allocation failed in the device builder");
 	}
@@ -2021,6 +1918,44 @@ int fmx_matrix_hot(const fmx_matrix *m, uint64_t *n_hot_cols, uint64_t *hot_entr
 	if (n_hot_cols) *n_hot_cols = p.n_hot;
 	if (hot_entries) *hot_entries = p.hot_entries;
 	if (scratch_bytes) *scratch_bytes = uint64_t(p.n_hot + 1) * kPanelBytes + uint64_t(p.n_partials) * kPartialStride * 8;
+	return FMX_OK;
+}
+
+int fmx_matrix_layout_digest(const fmx_matrix *m, int transpose, uint64_t *digest)
+{
+	if (!m || !m->a || !digest) return set_error(FMX_ERR_INVAL, "null argument");
+	const gpu_part *pp = transpose && !m->symmetric ? m->at.get() : m->a.get();
+	if (!pp) return set_error(FMX_ERR_INVAL, "the matrix has no transpose part");
+	const gpu_part &p = *pp;
+	if (p.streamed) return set_error(FMX_ERR_UNSUPPORTED, "a streamed matrix keeps its entry stream in host memory");
+	device_guard on_device(p.device);
+	if (!on_device.ok()) return set_error(FMX_ERR_CUDA, "cannot make device %d current", p.device);
+	uint64_t h = 0xcbf29ce484222325ull;          // FNV-1a, 64 bits
+	auto mix_host = [&](const void *q, size_t bytes) {
+		const unsigned char *c = static_cast<const unsigned char *>(q);
+		for (size_t i = 0; i < bytes; i++) { h ^= c[i]; h *= 0x100000001b3ull; }
+	};
+	std::vector<unsigned char> buf;
+	auto mix = [&](const void *dev, size_t bytes) -> int {
+		mix_host(&bytes, sizeof(bytes));
+		buf.resize(bytes);
+		if (bytes) CUDA_TRY(cudaMemcpy(buf.data(), dev, bytes, cudaMemcpyDeviceToHost));
+		mix_host(buf.data(), bytes);
+		return FMX_OK;
+	};
+	std::vector<range_t> rg(p.n_ranges);
+	if (p.n_ranges) CUDA_TRY(cudaMemcpy(rg.data(), p.ranges, rg.size() * sizeof(range_t), cudaMemcpyDeviceToHost));
+	uint64_t total = 0;
+	for (const range_t &r : rg) total = std::max<uint64_t>(total, uint64_t(r.e0) + r.len);
+	const size_t padded = size_t(total) + kStep;
+	const uint64_t counts[] = {p.nrows, p.ncols, p.nnz, p.n_hot, p.n_exact, p.n_ranges, p.n_heavy, p.n_long_heavy,
+			p.n_block_heavy, p.n_partials, p.hot_entries};
+	mix_host(counts, sizeof(counts));
+	for (int rc : {mix(p.ranges, rg.size() * sizeof(range_t)), mix(p.col, padded * sizeof(uint32_t)),
+			mix(p.val, p.esize ? padded * p.esize : 0), mix(p.heavy, size_t(p.n_heavy) * sizeof(heavy_row)),
+			mix(p.hot_col, size_t(p.n_hot) * sizeof(int32_t))})
+		if (rc) return rc;
+	*digest = h;
 	return FMX_OK;
 }
 

@@ -297,6 +297,13 @@ class sparse_matrix:
         check(lib.fmx_matrix_hot(self._h, *[C.byref(x) for x in v]))
         return tuple(x.value for x in v)
 
+    def layout_digest(self, transpose=False):
+        """64-bit digest of the resident layout of A (or of A^T): equal for two
+        builds exactly when they lay the matrix out identically."""
+        v = C.c_uint64()
+        check(lib.fmx_matrix_layout_digest(self._h, 1 if transpose else 0, C.byref(v)))
+        return v.value
+
     def transpose(self):
         h = C.c_void_p()
         check(lib.fmx_matrix_transpose(self._h, C.byref(h)))

@@ -244,6 +244,14 @@ int fmx_matrix_schedule(const fmx_matrix *m, uint64_t *n_light_rows, uint64_t *n
 int fmx_matrix_hot(const fmx_matrix *m, uint64_t *n_hot_cols, uint64_t *hot_entries,
                    uint64_t *scratch_bytes);
 
+/* A 64-bit FNV-1a digest of one resident orientation (transpose = 0: A,
+ * else A^T): the entry stream, values, ranges, heavy-row list, hot columns
+ * and the schedule counts.  Two builds of the same matrix (a host image
+ * through fmx_matrix_create, device edges through fmx_matrix_build_device)
+ * lay it out identically exactly when the digests agree.  Copies the layout
+ * to the host: a diagnostic, not for hot paths.  No reference counterpart. */
+int fmx_matrix_layout_digest(const fmx_matrix *m, int transpose, uint64_t *digest);
+
 /* ---- dense kernels of the block eigensolver --------------------------------
  * Tall-skinny products over n-row, row-major FP32 blocks of at most 64
  * columns (block_multi_vector::gemm / MvTransMv / MvNorm,
@@ -381,7 +389,9 @@ int fmx_gnn_free(fmx_gnn *g);
 /* Copy FMX_GNN_PARAMS floats in (resets the optimiser state) or out. */
 int fmx_gnn_set_params(fmx_gnn *g, const float *host);
 int fmx_gnn_get_params(const fmx_gnn *g, float *host);
-/* Z (n x 64 device floats) for matrix m with row scale s (NULL: none). */
+/* Z (n x 64 device floats, 16-byte aligned) for matrix m and its
+ * D^-1/2 row scale (fmx_na_scale; required: the degree feature is read
+ * back from it as 1 / s^2). */
 int fmx_gnn_features(const fmx_matrix *m, const float *row_scale, uint64_t seed,
                      float *Z, void *stream);
 /* Y (n x 16 device floats). */

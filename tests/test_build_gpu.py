@@ -50,8 +50,35 @@ def test_device_build_matches_host_build(torch_cuda, dedup, keep_self, weighted)
     host, dev = _pair(torch, src, dst, vals, n, dedup, keep_self)
     assert host.get_nnz() == dev.get_nnz()
     assert host.schedule() == dev.schedule()
+    # the GPU scheduler lays out both orientations byte for byte as the host one
+    assert host.layout_digest() == dev.layout_digest()
+    assert host.layout_digest(transpose=True) == dev.layout_digest(transpose=True)
     for k in (1, 16, 33):
         _same_products(torch, host, dev, k, torch.float32)
+
+
+def test_device_schedule_edge_rows(torch_cuda):
+    """Rows at the scheduler's boundaries: exactly 256 entries (summed whole),
+    257 (two chunks), 9 chunks (a warp each in the fixup), more than 64
+    chunks (a block each), empty rows first and last, FP64 values."""
+    torch = torch_cuda
+    rng = np.random.default_rng(11)
+    n = 50000
+    parts_s, parts_d = [], []
+    for row, deg in ((5, 20000), (6, 257), (7, 256), (8, 2100), (9, 1)):
+        parts_s.append(np.full(deg, row, np.uint32))
+        parts_d.append(rng.choice(np.arange(10, n - 10, dtype=np.uint32), deg, replace=False))
+    m = 300000
+    parts_s.append(rng.integers(10, n - 10, m).astype(np.uint32))
+    parts_d.append(rng.integers(0, n, m).astype(np.uint32))
+    src, dst = np.concatenate(parts_s), np.concatenate(parts_d)
+    vals = rng.uniform(-1, 1, len(src))
+    host, dev = _pair(torch, src, dst, vals, n, True, False, block=(4096, 4096))
+    assert host.schedule() == dev.schedule() and host.hot() == dev.hot()
+    assert host.layout_digest() == dev.layout_digest()
+    assert host.layout_digest(transpose=True) == dev.layout_digest(transpose=True)
+    for k in (1, 16):
+        _same_products(torch, host, dev, k, torch.float64)
 
 
 def test_device_rmat_matches_host_rmat(torch_cuda):
@@ -66,6 +93,8 @@ def test_device_rmat_matches_host_rmat(torch_cuda):
     assert np.array_equal(ds.cpu().numpy().view(np.uint32), s)
     dev = sparse_matrix.from_device_edges(ds, dd, nrows=n, ncols=n, dedup=True)
     assert host.get_nnz() == dev.get_nnz() and host.hot() == dev.hot()
+    assert host.schedule() == dev.schedule()
+    assert host.layout_digest() == dev.layout_digest()
     for dt in (torch.float32, torch.bfloat16):
         X = torch.randn((n, 16), device="cuda").to(dt)
         Y1 = torch.empty((n, 16), device="cuda")
