@@ -430,20 +430,27 @@ def eigen_measure(a, dev):
     for i in range(a.eig_sbm):
         inst = ws.sbm_instance(30_000_000 + i, solve=False)
         po, mo = ws.eigen_opts(inst.nev, 1e-6, "plain"), ws.eigen_opts(inst.nev, 1e-6, "mixed")
-        ms_p, rp = _timed_solve(torch, dev, lambda: compute_eigen(inst.op, True, po), reps=1)
+        ms_p, rp = _timed_solve(torch, dev, lambda: compute_eigen(inst.op, True, po), reps=3)
+        ms_m, rm = _timed_solve(torch, dev, lambda: compute_eigen(inst.op, True, mo), reps=3)
         ms_w, rw = _timed_solve(torch, dev, lambda: compute_eigen(inst.op, True, mo,
                                                                   X0=net.start_block(inst.op, 0, mo.block_size)),
-                                reps=1)
-        rows.append((ms_p, int(rp.status.spmm_calls), ms_w, int(rw.status.spmm_calls) + ws.SPMM_PER_START,
-                     int(rp.status.converged == inst.nev and rw.status.converged == inst.nev)))
+                                reps=3)
+        rows.append((ms_p, int(rp.status.spmm_calls), ms_m, int(rm.status.spmm_calls), ms_w,
+                     int(rw.status.spmm_calls) + ws.SPMM_PER_START,
+                     int(all(r.status.converged == inst.nev for r in (rp, rm, rw)))))
         del inst
     R = np.array(rows)
     out["sbm_heldout"] = {
         "graphs": a.eig_sbm, "n": "uniform 10k-200k", "blocks": "4-16 (nev = blocks)", "ratio": "5-20",
+        "timing": "median of 3 solves per graph and arm, after one warm-up, CUDA events around the solve",
         "plain_random_ms_median": round(float(np.median(R[:, 0])), 2),
-        "mixed_learned_ms_median": round(float(np.median(R[:, 2])), 2),
-        "plain_random_spmm_sum": int(R[:, 1].sum()), "mixed_learned_spmm_sum": int(R[:, 3].sum()),
-        "speedup_total_time": round(float(R[:, 0].sum() / R[:, 2].sum()), 3), "all_converged": int(R[:, 4].sum())}
+        "mixed_random_ms_median": round(float(np.median(R[:, 2])), 2),
+        "mixed_learned_ms_median": round(float(np.median(R[:, 4])), 2),
+        "plain_random_spmm_sum": int(R[:, 1].sum()), "mixed_random_spmm_sum": int(R[:, 3].sum()),
+        "mixed_learned_spmm_sum": int(R[:, 5].sum()),
+        "learned_vs_random_mixed_total_time": round(float(R[:, 2].sum() / R[:, 4].sum()), 3),
+        "learned_mixed_vs_random_plain_total_time": round(float(R[:, 0].sum() / R[:, 4].sum()), 3),
+        "all_converged": int(R[:, 6].sum())}
     return out
 
 
@@ -626,6 +633,17 @@ def dense_measure(dev, peak, n=1 << 22, b=16, steps=20):
         out[f"gram_{names[prec]}"] = {"us": round(us, 1), "frac": round(n * 2 * b * 4 / us / 1e3 / peak, 4),
                                      "rel_err": float(f"{float((G.double() - ref).abs().max() / ref.abs().max()):.2e}")}
     out["tensor_core_errors"] = int(err.item())
+    # the Rayleigh-Ritz eigenproblem of the solver (FP64 Jacobi) at the
+    # block sizes the eigen and large configurations use
+    jac = {}
+    for bb in (16, 24):
+        A = torch.randn((bb, bb), generator=g, device=dev, dtype=torch.float64)
+        H = (A + A.T).contiguous()
+        wv = torch.empty(bb, dtype=torch.float64, device=dev)
+        V = torch.empty((bb, bb), dtype=torch.float64, device=dev)
+        jac[f"b{bb}_us"] = round(timed(lambda: _lib.lib.fmx_dense_sym_eig(H.data_ptr(), bb, wv.data_ptr(), V.data_ptr(),
+                                                                         st)), 1)
+    out["sym_eig"] = jac
     del X, W, B, Y
     torch.cuda.empty_cache()
     return out

@@ -1219,6 +1219,136 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_eig_kernel(const double
 	for (int i = t; i < b * b; i += blockDim.x) V[i] = Q[i / b][order[i % b]];
 }
 
+// The same decomposition for b <= 32 on NW <= 4 warps (one warp for b <= 16:
+// warp barriers only).  A step applies each rotation to rows and columns at
+// once: with index i in pair (p, q) and new row i = k1(i) A[p] + k2(i) A[q]
+// (k = (c, -s) for i = p, (s, c) for i = q),
+//   A'[i][j] = sum_{x,y} k_x(i) k_y(j) A[r_x(i)][r_y(j)],
+//   Q'[i][j] = sum_y Q[i][r_y(j)] k_y(j),
+// and a rotated pair's own entries are set exactly: a_pp - t a_pq,
+// a_qq + t a_pq and 0.  Each thread owns KP fixed elements (i, j), computed
+// into registers between two barriers.
+constexpr int kJacobiSmallMax = 32;
+
+template <int NW>
+__device__ __forceinline__ void jac_sync()
+{
+	if constexpr (NW == 1) __syncwarp();
+	else __syncthreads();
+}
+
+template <int NW, int KP>
+__global__ void __launch_bounds__(32 * NW) jacobi_small_kernel(const double *__restrict__ H, int b,
+		double *__restrict__ w, double *__restrict__ V, int max_sweeps)
+{
+	constexpr int NT = 32 * NW;
+	__shared__ double A[kJacobiSmallMax][kJacobiSmallMax + 1], Q[kJacobiSmallMax][kJacobiSmallMax + 1];
+	__shared__ double k1[kJacobiSmallMax], k2[kJacobiSmallMax], dg[kJacobiSmallMax];
+	__shared__ int r1[kJacobiSmallMax], r2[kJacobiSmallMax], mate[kJacobiSmallMax], order[kJacobiSmallMax];
+	__shared__ double red[2][NW];
+	const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+	const int m = (b + 1) & ~1;                       // even size (pad with a zero row/column)
+	const int half = m / 2, mm = m * m;
+	int ei[KP], ej[KP];
+#pragma unroll
+	for (int u = 0; u < KP; u++) {
+		const int e = t + NT * u;
+		ei[u] = e < mm ? e / m : -1;
+		ej[u] = e < mm ? e % m : 0;
+	}
+	for (int e = t; e < mm; e += NT) {
+		const int r = e / m, c = e % m;
+		A[r][c] = (r < b && c < b) ? 0.5 * (H[r * b + c] + H[c * b + r]) : 0.0;
+		Q[r][c] = (r == c) ? 1.0 : 0.0;
+	}
+	if (t < kJacobiSmallMax) order[t] = t;            // complete even if the padding is not recognised
+	jac_sync<NW>();
+	for (int sweep = 0; sweep < max_sweeps; sweep++) {
+		double so = 0, sd = 0;
+#pragma unroll
+		for (int u = 0; u < KP; u++) {
+			if (ei[u] < 0) continue;
+			const double v = A[ei[u]][ej[u]] * A[ei[u]][ej[u]];
+			if (ei[u] == ej[u]) sd += v; else so += v;
+		}
+		for (int o = 16; o > 0; o >>= 1) {
+			so += __shfl_xor_sync(0xffffffffu, so, o);
+			sd += __shfl_xor_sync(0xffffffffu, sd, o);
+		}
+		if constexpr (NW > 1) {
+			if (lane == 0) { red[0][wid] = so; red[1][wid] = sd; }
+			__syncthreads();
+			so = 0; sd = 0;
+			for (int i = 0; i < NW; i++) { so += red[0][i]; sd += red[1][i]; }
+			__syncthreads();
+		}
+		if (so / (sd > 0 ? sd : 1.0) < 1e-30) break;
+		for (int step = 0; step < m - 1; step++) {
+			if (t < half) {
+				// round-robin tournament pairing of 0..m-1
+				int a = t == 0 ? 0 : 1 + (t - 1 + step) % (m - 1);
+				int q = 1 + (m - 2 - t + step) % (m - 1);
+				if (a > q) { const int x = a; a = q; q = x; }
+				const double app = A[a][a], aqq = A[q][q], apq = A[a][q];
+				double c = 1, sn = 0, tt = 0;
+				if (fabs(apq) > 1e-300) {
+					const double tau = (aqq - app) / (2 * apq);
+					tt = (tau >= 0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1 + tau * tau));
+					c = 1 / sqrt(1 + tt * tt);
+					sn = tt * c;
+				}
+				r1[a] = a; r2[a] = q; k1[a] = c; k2[a] = -sn; dg[a] = -tt * apq; mate[a] = q;
+				r1[q] = a; r2[q] = q; k1[q] = sn; k2[q] = c; dg[q] = tt * apq; mate[q] = a;
+			}
+			jac_sync<NW>();
+			double na[KP], nq[KP];
+#pragma unroll
+			for (int u = 0; u < KP; u++) {
+				const int i = ei[u], j = ej[u];
+				if (i < 0) continue;
+				const int ja = r1[j], jb = r2[j];
+				const double ya = k1[j], yb = k2[j];
+				nq[u] = Q[i][ja] * ya + Q[i][jb] * yb;
+				if (i == j) {
+					na[u] = A[i][i] + dg[i];
+				} else if (mate[i] == j) {
+					na[u] = 0.0;
+				} else {
+					const int ia = r1[i], ib = r2[i];
+					const double xa = k1[i], xb = k2[i];
+					na[u] = xa * (A[ia][ja] * ya + A[ia][jb] * yb) + xb * (A[ib][ja] * ya + A[ib][jb] * yb);
+				}
+			}
+			jac_sync<NW>();
+#pragma unroll
+			for (int u = 0; u < KP; u++) {
+				if (ei[u] < 0) continue;
+				A[ei[u]][ej[u]] = na[u];
+				Q[ei[u]][ej[u]] = nq[u];
+			}
+			jac_sync<NW>();
+		}
+	}
+	// descending order of the b real eigenvalues (the padding one, if any, is dropped)
+	if (t < 32) {
+		const bool real = lane < m && !((m != b) && (fabs(Q[b][lane]) > 0.5));
+		const unsigned rmask = __ballot_sync(0xffffffffu, real);
+		const double mine = lane < m ? A[lane][lane] : 0.0;
+		if (real) {
+			int rank = 0;
+			for (int j = 0; j < m; j++) {
+				if (!((rmask >> j) & 1u)) continue;
+				const double o = A[j][j];
+				rank += (o > mine) || (o == mine && j < lane);
+			}
+			if (rank < b) order[rank] = lane;
+		}
+	}
+	jac_sync<NW>();
+	for (int i = t; i < b; i += NT) w[i] = A[order[i]][order[i]];
+	for (int i = t; i < b * b; i += NT) V[i] = Q[i / b][order[i % b]];
+}
+
 int sms(int device)
 {
 	int s = 0;
@@ -1367,6 +1497,16 @@ int fmx_dense_sym_eig(const double *H, int b, double *w, double *V, void *stream
 {
 	if (!H || !w || !V) return set_error(FMX_ERR_INVAL, "null argument");
 	if (b < 1 || b > 64) return set_error(FMX_ERR_UNSUPPORTED, "b in 1..64");
+	if (b <= 16) {
+		jacobi_small_kernel<1, 8><<<1, 32, 0, static_cast<cudaStream_t>(stream)>>>(H, b, w, V, 30);
+		DCUDA_TRY(cudaGetLastError());
+		return FMX_OK;
+	}
+	if (b <= kJacobiSmallMax) {
+		jacobi_small_kernel<4, 8><<<1, 128, 0, static_cast<cudaStream_t>(stream)>>>(H, b, w, V, 30);
+		DCUDA_TRY(cudaGetLastError());
+		return FMX_OK;
+	}
 	const int smem = 2 * 64 * 65 * int(sizeof(double));
 	DCUDA_TRY(cudaFuncSetAttribute(jacobi_eig_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
 	jacobi_eig_kernel<<<1, kJacobiThreads, smem, static_cast<cudaStream_t>(stream)>>>(H, b, w, V, 30);

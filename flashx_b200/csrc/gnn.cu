@@ -2,7 +2,8 @@
 // maps vertex features to a 16-column start block.  It has no counterpart in
 // the reference; it feeds fmx_eigen_solve's X0.
 //
-//   F  (n x 16)   standardised log(1 + degree), then 15 N(0,1) channels
+//   F  (n x 16)   standardised log(1 + degree) (the degree read back from the
+//                 D^-1/2 scale), then 15 N(0,1) channels
 //   Z  (n x 64)   [F, A_s F, A_s^2 F, A_s^3 F]      (A_s = D^-1/2 A D^-1/2)
 //   H  (n x 64)   relu(Z W1 + b1)                   layer 1, hidden 64
 //   Y  (n x 16)   A_s (H W2)                        layer 2
@@ -66,17 +67,19 @@ __device__ __forceinline__ uint64_t mix64(uint64_t z)
 	return z ^ (z >> 31);
 }
 
-// uniform in (0, 1] from 53 random bits
-__device__ __forceinline__ double unit53(uint64_t u) { return (double(u >> 11) + 1.0) * (1.0 / 9007199254740992.0); }
 
-// per-CTA sum and sum of squares of log(1 + d) over the rows (FP64)
-__global__ void __launch_bounds__(kThreads) logdeg_stats_kernel(const float *__restrict__ d, int64_t n,
+// log(1 + degree) of a row from its D^-1/2 scale s (0 for an empty row):
+// degree = 1 / s^2, within a few ulps of the row sum the scale came from
+__device__ __forceinline__ float log_degree(float s) { return s > 0.f ? log1pf(1.f / (s * s)) : 0.f; }
+
+// per-CTA sum and sum of squares of log(1 + degree) over the rows (FP64)
+__global__ void __launch_bounds__(kThreads) logdeg_stats_kernel(const float *__restrict__ scale, int64_t n,
 		double *__restrict__ part)
 {
 	__shared__ double s1[kThreads], s2[kThreads];
 	double a = 0, c = 0;
 	for (int64_t i = blockIdx.x * int64_t(kThreads) + threadIdx.x; i < n; i += int64_t(gridDim.x) * kThreads) {
-		const double v = log1p(double(d[i]));
+		const double v = log_degree(scale[i]);
 		a += v;
 		c += v * v;
 	}
@@ -96,43 +99,56 @@ __global__ void __launch_bounds__(kThreads) logdeg_stats_kernel(const float *__r
 	}
 }
 
-// F = Z[:, 0:16]: channel 0 the standardised log-degree, channels 1..15
-// N(0, 1) by the Box-Muller transform of counter-based uniforms
-__global__ void features_kernel(const float *__restrict__ d, int64_t n, const double *__restrict__ part, int nparts,
-		uint64_t seed, float *__restrict__ Z)
+// F = Z[:, 0:16], a thread per row: channel 0 the standardised log-degree,
+// channels 1..15 N(0, 1), pairs of them by the Box-Muller transform of two
+// counter-based uniforms (cos and sin of the same pair)
+__global__ void features_kernel(const float *__restrict__ scale, int64_t n, const double *__restrict__ part,
+		int nparts, uint64_t seed, float *__restrict__ Z)
 {
-	__shared__ double mean, inv_std;
+	__shared__ float mean, inv_std;
 	if (threadIdx.x == 0) {
 		double a = 0, c = 0;
 		for (int p = 0; p < nparts; p++) {
 			a += part[2 * p];
 			c += part[2 * p + 1];
 		}
-		mean = a / double(n > 0 ? n : 1);
-		const double var = c / double(n > 0 ? n : 1) - mean * mean;
-		inv_std = var > 1e-20 ? 1.0 / sqrt(var) : 1.0;
+		const double m = a / double(n > 0 ? n : 1);
+		const double var = c / double(n > 0 ? n : 1) - m * m;
+		mean = float(m);
+		inv_std = float(var > 1e-20 ? 1.0 / sqrt(var) : 1.0);
 	}
 	__syncthreads();
-	for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n * kF; i += int64_t(gridDim.x) * blockDim.x) {
-		const int64_t row = i / kF;
-		const int ch = int(i % kF);
-		float v;
-		if (ch == 0) {
-			v = float((log1p(double(d[row])) - mean) * inv_std);
-		} else {
-			const uint64_t key = seed * 0x9E3779B97F4A7C15ull ^ (uint64_t(row) * kF + uint64_t(ch));
-			const double u1 = unit53(mix64(key)), u2 = unit53(mix64(key ^ 0xD1B54A32D192ED03ull));
-			v = float(sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2));
+	for (int64_t row = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; row < n; row += int64_t(gridDim.x) * blockDim.x) {
+		float f[kF];
+		f[0] = (log_degree(scale[row]) - mean) * inv_std;
+#pragma unroll
+		for (int q = 0; q < kF / 2; q++) {
+			const uint64_t key = seed * 0x9E3779B97F4A7C15ull ^ (uint64_t(row) * kF + uint64_t(q));
+			const uint64_t z = mix64(key);
+			const float u1 = (float(uint32_t(z) >> 8) + 1.f) * (1.f / 16777216.f);     // (0, 1]
+			const float u2 = float(uint32_t(z >> 32) >> 8) * (1.f / 16777216.f);       // [0, 1)
+			const float r = sqrtf(-2.f * logf(u1));
+			float sn, cs;
+			sincospif(2.f * u2, &sn, &cs);
+			if (2 * q + 1 < kF) f[2 * q + 1] = r * cs;
+			if (2 * q + 2 < kF) f[2 * q + 2] = r * sn;
 		}
-		Z[row * kZ + ch] = v;
+		float4 *o = reinterpret_cast<float4 *>(Z + row * kZ);
+#pragma unroll
+		for (int v = 0; v < kF / 4; v++) o[v] = make_float4(f[4 * v], f[4 * v + 1], f[4 * v + 2], f[4 * v + 3]);
 	}
 }
 
-// H = relu(H + b1) in place (n x kH)
-__global__ void bias_relu_kernel(float *__restrict__ H, const float *__restrict__ b1, int64_t n)
+// H = relu(H + b1) in place (n x kH, 16-byte vectors)
+__global__ void bias_relu_kernel(float4 *__restrict__ H, const float4 *__restrict__ b1, int64_t n)
 {
-	for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n * kH; i += int64_t(gridDim.x) * blockDim.x)
-		H[i] = fmaxf(H[i] + b1[i % kH], 0.f);
+	for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n * (kH / 4); i += int64_t(gridDim.x) * blockDim.x) {
+		const float4 b = b1[uint32_t(i) % uint32_t(kH / 4)];
+		float4 h = H[i];
+		h.x = fmaxf(h.x + b.x, 0.f); h.y = fmaxf(h.y + b.y, 0.f);
+		h.z = fmaxf(h.z + b.z, 0.f); h.w = fmaxf(h.w + b.w, 0.f);
+		H[i] = h;
+	}
 }
 
 // dH *= (H > 0) in place; part[cta][j] = the CTA's column sums of the masked
@@ -285,11 +301,6 @@ __global__ void adam_kernel(float *__restrict__ p, float *__restrict__ m, float 
 	}
 }
 
-__global__ void fill_kernel(float *p, int64_t n, float v)
-{
-	for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) p[i] = v;
-}
-
 int sm_count()
 {
 	int dev = 0, s = 0;
@@ -362,7 +373,8 @@ int forward(const fmx_gnn *g, const fmx_matrix *m, const float *scale, const flo
 		float *H, float *Z2, float *Y, cudaStream_t st)
 {
 	G_TRY(fmx_dense_gemm(precision, Z, kZ, n, kZ, g->p + kOffW1, kH, kH, H, kH, g->err, st));
-	bias_relu_kernel<<<grid_for(n * kH), kThreads, 0, st>>>(H, g->p + kOffB1, n);
+	bias_relu_kernel<<<grid_for(n * kH / 4), kThreads, 0, st>>>(reinterpret_cast<float4 *>(H),
+			reinterpret_cast<const float4 *>(g->p + kOffB1), n);
 	GCUDA_TRY(cudaGetLastError());
 	G_TRY(fmx_dense_gemm(precision, H, kH, n, kH, g->p + kOffW2, kOut, kOut, Z2, kOut, g->err, st));
 	G_TRY(fmx_spmm(m, FMX_F32, Z2, kOut, FMX_F32, Y, kOut, kOut, scale, scale, st));
@@ -457,24 +469,19 @@ int fmx_gnn_get_params(const fmx_gnn *g, float *host)
 
 int fmx_gnn_features(const fmx_matrix *m, const float *scale, uint64_t seed, float *Z, void *stream)
 {
-	if (!m || !Z) return set_error(FMX_ERR_INVAL, "null argument");
+	if (!m || !Z || !scale) return set_error(FMX_ERR_INVAL, "null argument");
+	if (reinterpret_cast<uintptr_t>(Z) % 16) return set_error(FMX_ERR_INVAL, "Z must be 16-byte aligned");
 	int64_t n = 0;
 	G_TRY(check_matrix(m, &n));
 	cudaStream_t st = static_cast<cudaStream_t>(stream);
 	scratch s;
 	s.st = st;
-	float *ones = nullptr, *deg = nullptr;
 	double *part = nullptr;
 	const int parts = int(grid_for(n));
-	G_TRY(s.get(&ones, size_t(n)));
-	G_TRY(s.get(&deg, size_t(n)));
 	G_TRY(s.get(&part, size_t(2 * parts)));
-	fill_kernel<<<grid_for(n), kThreads, 0, st>>>(ones, n, 1.f);
+	logdeg_stats_kernel<<<parts, kThreads, 0, st>>>(scale, n, part);
 	GCUDA_TRY(cudaGetLastError());
-	G_TRY(fmx_spmm(m, FMX_F32, ones, 1, FMX_F32, deg, 1, 1, nullptr, nullptr, st));
-	logdeg_stats_kernel<<<parts, kThreads, 0, st>>>(deg, n, part);
-	GCUDA_TRY(cudaGetLastError());
-	features_kernel<<<grid_for(n * kF), kThreads, 0, st>>>(deg, n, part, parts, seed, Z);
+	features_kernel<<<grid_for(n), kThreads, 0, st>>>(scale, n, part, parts, seed, Z);
 	GCUDA_TRY(cudaGetLastError());
 	for (int h = 1; h <= kHops; h++)
 		G_TRY(fmx_spmm(m, FMX_F32, Z + (h - 1) * kF, kZ, FMX_F32, Z + h * kF, kZ, kF, scale, scale, st));

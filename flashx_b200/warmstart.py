@@ -190,6 +190,57 @@ def compare_starts(net, inst, tol=1e-6, precision="plain", seed=0):
             "converged": bool(cold.status.converged == inst.nev and warm.status.converged == inst.nev)}
 
 
+def _median_solve_ms(fn, reps):
+    """Median time (ms, CUDA events around the call) of `reps` calls of fn
+    after one untimed call, and the last result."""
+    import torch
+    fn()
+    times, res = [], None
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        res = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    return float(np.median(times)), res
+
+
+def evaluate(net, n_test=200, n_range=(10000, 200000), tol=1e-6, seed=0, reps=3, log=None):
+    """Three starts on `n_test` held-out SBM graphs (the seeds `study` holds
+    out): the plain solver from a random block, the mixed solver from a
+    random block, and the mixed solver from the network's block (its 4 SpMMs
+    and its time included).  Returns per-graph rows and totals."""
+    rows = []
+    for s in range(n_test):
+        inst = sbm_instance(seed * 1000003 + 10_000_000 + s, n_range=n_range, tol=tol, solve=False)
+        po, mo = eigen_opts(inst.nev, tol, "plain"), eigen_opts(inst.nev, tol, "mixed")
+        tp, rp = _median_solve_ms(lambda: compute_eigen(inst.op, True, po), reps)
+        tm, rm = _median_solve_ms(lambda: compute_eigen(inst.op, True, mo), reps)
+        tw, rw = _median_solve_ms(lambda: compute_eigen(inst.op, True, mo, X0=net.start_block(inst.op, s, mo.block_size)),
+                                  reps)
+        rows.append({"n": inst.n, "blocks": inst.nblocks, "ratio": round(inst.ratio, 2),
+                     "ms_plain": round(tp, 3), "ms_mixed": round(tm, 3), "ms_learned": round(tw, 3),
+                     "spmm_plain": int(rp.status.spmm_calls), "spmm_mixed": int(rm.status.spmm_calls),
+                     "spmm_learned": int(rw.status.spmm_calls) + SPMM_PER_START,
+                     "converged": bool(all(r.status.converged == inst.nev for r in (rp, rm, rw)))})
+        if log and (s + 1) % 50 == 0:
+            log(f"evaluated {s + 1} held-out graphs")
+        del inst
+    ok = [r for r in rows if r["converged"]]
+    med = lambda k: float(np.median([r[k] for r in ok])) if ok else float("nan")
+    tot = lambda k: float(sum(r[k] for r in ok))
+    return {"n_test": n_test, "converged": len(ok), "reps": reps,
+            "median_ms": {k: round(med("ms_" + k), 3) for k in ("plain", "mixed", "learned")},
+            "total_ms": {k: round(tot("ms_" + k), 1) for k in ("plain", "mixed", "learned")},
+            "median_spmm": {k: med("spmm_" + k) for k in ("plain", "mixed", "learned")},
+            "total_spmm": {k: int(tot("spmm_" + k)) for k in ("plain", "mixed", "learned")},
+            "learned_fewer_spmm_than_mixed": int(sum(r["spmm_learned"] < r["spmm_mixed"] for r in ok)),
+            "learned_faster_than_mixed": int(sum(r["ms_learned"] < r["ms_mixed"] for r in ok)),
+            "rows": rows}
+
+
 def study(n_train=2000, n_test=200, epochs=4, lr=3e-3, n_range=(10000, 200000), precision="plain", tol=1e-6,
           weights_out=None, seed=0, log=print):
     """Train on `n_train` generated SBM graphs (n uniform in n_range, 4-16
@@ -236,7 +287,17 @@ if __name__ == "__main__":
     ap.add_argument("--precision", default="plain", choices=["plain", "mixed"])
     ap.add_argument("--weights", default=None, help="write the trained weights (flat little-endian float32)")
     ap.add_argument("--out", default=None, help="write the summary as JSON")
+    ap.add_argument("--eval-only", action="store_true",
+                    help="load --weights and compare plain-random, mixed-random and mixed-learned starts on the "
+                         "--test held-out graphs")
     a = ap.parse_args()
+    if a.eval_only:
+        res = evaluate(warm_start_net.load(a.weights), a.test, n_range=(a.nmin, a.nmax), log=print)
+        print(json.dumps({k: v for k, v in res.items() if k != "rows"}), flush=True)
+        if a.out:
+            with open(a.out, "w") as f:
+                json.dump(res, f)
+        raise SystemExit(0)
     res = study(a.train, a.test, a.epochs, n_range=(a.nmin, a.nmax), precision=a.precision, weights_out=a.weights)
     brief = {k: v for k, v in res.items() if k != "rows"}
     print(json.dumps(brief), flush=True)

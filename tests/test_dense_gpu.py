@@ -110,7 +110,7 @@ def test_chol_inv(torch_cuda, b):
     assert int(info.item()) > 0
 
 
-@pytest.mark.parametrize("b", [1, 2, 7, 16, 32, 48, 64])
+@pytest.mark.parametrize("b", [1, 2, 7, 16, 24, 31, 32, 33, 48, 64])
 def test_sym_eig(torch_cuda, b):
     torch = torch_cuda
     g = torch.Generator(device="cuda").manual_seed(100 + b)

@@ -101,6 +101,24 @@ def test_gradient_matches_finite_differences(torch_cuda):
     net.set_params(p0)
 
 
+def test_features_match_their_definition(torch_cuda):
+    """Z = [F, N F, N^2 F, N^3 F] with F[:, 0] the standardised log(1 + degree)
+    and F[:, 1:] N(0, 1) channels (N = D^-1/2 A D^-1/2, FP64 on the CPU)."""
+    torch = torch_cuda
+    g = _graph(torch, n=6000, B=6)
+    Z = warm_start_net.features(g.op, 5).double().cpu().numpy()
+    A = g.N
+    sc = g.op.scale.double().cpu().numpy()
+    ld = np.where(sc > 0, np.log1p(1.0 / np.maximum(sc, 1e-30) ** 2), 0.0)
+    np.testing.assert_allclose(Z[:, 0], (ld - ld.mean()) / ld.std(), atol=1e-4)
+    R = Z[:, 1:16].ravel()
+    assert abs(R.mean()) < 0.02 and abs(R.std() - 1.0) < 0.02
+    F = Z[:, :16]
+    for h in range(1, 4):
+        F = A @ F
+        np.testing.assert_allclose(Z[:, 16 * h:16 * (h + 1)], F, atol=1e-4 * max(1.0, float(np.abs(F).max())))
+
+
 def test_params_roundtrip_and_determinism(torch_cuda, tmp_path):
     torch = torch_cuda
     g = _graph(torch, n=2000)
