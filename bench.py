@@ -287,6 +287,68 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+class NvmlSampler:
+    """SM clock and clock-event reasons polled through NVML every ~1 ms while
+    the timed region runs (a region of tens of ms gets tens of samples; the
+    nvidia-smi sampler's 200 ms period would see at most one).  Falls back to
+    ClockSampler when NVML is unavailable."""
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40, "sw_power_cap": 0x4}
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.samples = []
+        self.fallback = None
+        self.stop_flag = threading.Event()
+
+    def _handle(self, nv):
+        import torch
+        try:
+            pr = torch.cuda.get_device_properties(self.gpu)
+            bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+            return nv.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return nv.nvmlDeviceGetHandleByIndex(self.gpu)
+
+    def start(self):
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            self.nv = nv
+            self.h = self._handle(nv)
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM))
+        except Exception:
+            self.fallback = ClockSampler(self.gpu)
+            self.fallback.start()
+            return
+        self.th = threading.Thread(target=self._poll, daemon=True)
+        self.th.start()
+
+    def _poll(self):
+        nv = self.nv
+        while not self.stop_flag.is_set():
+            try:
+                mhz = float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+                reasons = int(nv.nvmlDeviceGetCurrentClocksEventReasons(self.h))
+                self.samples.append((mhz, reasons))
+            except Exception:
+                pass
+            time.sleep(0.001)
+
+    def stop(self):
+        if self.fallback is not None:
+            return self.fallback.stop()
+        self.stop_flag.set()
+        self.th.join(timeout=5)
+        try:
+            self.nv.nvmlShutdown()
+        except Exception:
+            pass
+        sm = [x for x, _ in self.samples]
+        reasons = sorted(nm for nm, bit in self.REASONS.items() if any(r & bit for _, r in self.samples))
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                "samples": len(sm), "sampler": "NVML, every ~1 ms during the timed region"}
+
+
 def read_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -828,8 +890,7 @@ def main():
     torch.cuda.synchronize(dev)
 
     # -- timed region --
-    clocks = ClockSampler(local)
-    clocks.start()
+    clocks = NvmlSampler(local)
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
     if world > 1:
@@ -837,6 +898,7 @@ def main():
     torch.cuda.synchronize(dev)
     t_begin = torch.cuda.Event(enable_timing=True)
     t_end = torch.cuda.Event(enable_timing=True)
+    clocks.start()
     t_begin.record(stream)
     for i in range(a.steps):
         starts[i].record(stream)
