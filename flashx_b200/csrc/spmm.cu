@@ -38,19 +38,20 @@
 // Why the hot pack: the X gathers of an R-MAT graph are random 64-byte reads
 // that mostly miss the L2, and a hot row shares its 128-byte line with a cold
 // one.  Packing the highest in-degree rows (about 87% of the gathers at scale
-// 24) two to a line, read with an L2 evict_last hint while the cold rows and
-// the streams use evict_first, keeps them resident.
+// 24) two to a line keeps them in a range the L2 can hold.
 //
-// Execution: a persistent grid.  A warp is split into R = floor(32/G) lane
-// groups of G lanes; a lane loads 16 bytes of an X row, so G lanes cover a
-// row of k elements.  Lane groups take ranges round-robin and walk them as a
-// stream of entries in aligned steps of U (4 or 8): a step loads its column
-// ids with 16-byte loads, issues its U gathers together with the next step's
-// column-id loads, then adds them up in entry order; when an entry closes a
-// row the group stores that row (the range's first row plus the rows closed
-// before it).  Every row of up to kExactMax
-// entries is summed by one group in the reference's order (bit-identical
-// results).  No atomics: every output row is written exactly once.
+// Execution: persistent grids whose lane groups take ranges round-robin and
+// walk them as a stream of entries in aligned steps; when an entry closes a
+// row, the group stores that row (the range's first row plus the rows closed
+// before it).  Every row of up to kExactMax entries is summed by one group in
+// the reference's order (bit-identical results).  No atomics: every output
+// row is written exactly once.  Three row kernels share that scheme:
+//   spmm_wide_kernel  FP32 panels of 32, 64 or 128 bytes: a lane owns 32 bytes
+//                     of each gathered row; 8 column ids per 32-byte load
+//   spmm_kernel       16-byte lanes (BF16, FP64, integer and odd widths),
+//                     with L2 evict_last hints on hot-pack gathers and
+//                     evict_first on cold rows
+//   spmv_kernel       k = 1: a warp per range, gathers staged in shared memory
 #include "fmx_internal.h"
 
 #include <cuda_runtime.h>
@@ -1353,7 +1354,8 @@ static int launch_t(const gpu_part &p, spmm_args a, bool sin, bool sout, cudaStr
 		CUDA_TRY(cudaGetLastError());
 	}
 	int rc = over_slices(p, a, st, [&](const spmm_args &sa) -> int {
-		if constexpr (std::is_same<A, float>::value && sizeof(XT) == 4 &&
+		if constexpr (std::is_same<A, float>::value &&
+				(sizeof(XT) == 4 || (sizeof(YT) == 2 && std::is_void<WT>::value)) &&
 				(std::is_same<WT, void>::value || std::is_same<WT, float>::value)) {
 			if (wide) {
 				if (sin && sout) return launch_wide<XT, YT, WT, true, true>(p, sa, st);
@@ -1443,7 +1445,13 @@ static int run_typed(const gpu_part &p, const void *X, int64_t ldx, void *Y, int
 		// (BF16 rows of 16 elements take the 16-byte lanes: measured at R-MAT
 		// scale 24, k = 16, one 32-byte lane per row loads an index group per
 		// lane and ran 2.2 ms against 1.8 ms)
-		const bool wide = std::is_same<A, float>::value && sizeof(XT) == 4 && vec_ok && (kp * sizeof(XT)) % 32 == 0 &&
+		// FP32, and unweighted BF16 with BF16 output (the eigensolver's
+		// correction SpMMs: 0.82 against 0.89 ms per call at scale 22,
+		// k = 16); BF16 into FP32 and weighted BF16 keep the 16-byte lanes,
+		// where the wider accumulators spill
+		constexpr bool kWideBf16 = sizeof(YT) == 2 && std::is_void<WT>::value;
+		const bool wide = std::is_same<A, float>::value && (sizeof(XT) == 4 || kWideBf16) && vec_ok &&
+				(kp * sizeof(XT)) % 32 == 0 &&
 				(ldx * sizeof(XT)) % 32 == 0 && (ldy * sizeof(YT)) % 32 == 0 && aligned32(a.X) && aligned32(a.Y);
 		if (wide) {
 			a.G = int(kp * sizeof(XT) / 32);     // 1, 2 or 4

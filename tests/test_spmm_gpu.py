@@ -158,6 +158,18 @@ def test_row_scales(torch_cuda):
         R = oracle.spmm(idx, mat, (X * s_in[:, None]).astype(dt)) * s_out[:, None]
         np.testing.assert_allclose(Y, R, rtol=RTOL if dt == np.float32 else 1e-12,
                                    atol=(RTOL if dt == np.float32 else 1e-12) * np.abs(R).max())
+    # BF16 in and out with both scales (the eigensolver's correction SpMMs):
+    # FP32 accumulation of the BF16-rounded operand, one BF16 rounding at the end
+    s_in = rng.uniform(0.1, 2.0, n).astype(np.float32)
+    s_out = rng.uniform(0.1, 2.0, n).astype(np.float32)
+    for k in (16, 32, 8):
+        xb = torch.from_numpy(rng.standard_normal((n, k)).astype(np.float32)).to(torch.bfloat16).cuda()
+        yb = torch.empty((n, k), dtype=torch.bfloat16, device="cuda")
+        assert m.multiply(xb, yb, torch.from_numpy(s_in).cuda(), torch.from_numpy(s_out).cuda())
+        Xr = xb.float().cpu().numpy()
+        R = (oracle.spmm(idx, mat, (Xr * s_in[:, None]).astype(np.float32)) * s_out[:, None]).astype(np.float32)
+        got = yb.float().cpu().numpy()
+        np.testing.assert_allclose(got, R, rtol=1e-2, atol=1e-2 * np.abs(R).max())
 
 
 def test_asymmetric_transpose(torch_cuda):
