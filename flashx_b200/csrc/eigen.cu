@@ -139,6 +139,37 @@ __device__ __forceinline__ void st4(__nv_bfloat16 *p, float4 v)
 	*reinterpret_cast<uint2 *>(p) = u;
 }
 
+__device__ __forceinline__ void ld8(const float *p, float (&t)[8])
+{
+	const float4 a = ld4(p), c = ld4(p + 4);
+	t[0] = a.x; t[1] = a.y; t[2] = a.z; t[3] = a.w; t[4] = c.x; t[5] = c.y; t[6] = c.z; t[7] = c.w;
+}
+__device__ __forceinline__ void ld8(const __nv_bfloat16 *p, float (&t)[8])
+{
+	const uint4 u = *reinterpret_cast<const uint4 *>(p);        // element 0 in the low half
+	const uint32_t w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+	for (int q = 0; q < 4; q++) {
+		t[2 * q] = __uint_as_float(w[q] << 16);
+		t[2 * q + 1] = __uint_as_float(w[q] & 0xffff0000u);
+	}
+}
+__device__ __forceinline__ void st8(float *p, const float (&v)[8])
+{
+	st4(p, make_float4(v[0], v[1], v[2], v[3]));
+	st4(p + 4, make_float4(v[4], v[5], v[6], v[7]));
+}
+__device__ __forceinline__ void st8(__nv_bfloat16 *p, const float (&v)[8])
+{
+	uint32_t w[4];
+#pragma unroll
+	for (int q = 0; q < 4; q++) {
+		__nv_bfloat162 h = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
+		memcpy(&w[q], &h, 4);
+	}
+	*reinterpret_cast<uint4 *>(p) = make_uint4(w[0], w[1], w[2], w[3]);
+}
+
 template <class WT, class ET, class PT, class OT>
 __global__ void corr_kernel(const WT *__restrict__ W, const ET *__restrict__ E, const PT *__restrict__ P,
 		const float *__restrict__ R, const float *__restrict__ X, OT *__restrict__ O, int64_t count, int b,
@@ -146,6 +177,44 @@ __global__ void corr_kernel(const WT *__restrict__ W, const ET *__restrict__ E, 
 {
 	const bool pow2 = (b & (b - 1)) == 0;
 	const int64_t tstride = int64_t(gridDim.x) * blockDim.x;
+	if ((b & 7) == 0) {
+		// eight consecutive elements of one row per thread (16-byte loads of
+		// BF16 blocks); each element's arithmetic is the four-wide path's
+		for (int64_t i8 = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i8 < count / 8; i8 += tstride) {
+			const int64_t i = 8 * i8;
+			const int col = pow2 ? int(i & (b - 1)) : int(i % b);
+			float v[8], t[8];
+#pragma unroll
+			for (int q = 0; q < 8; q++) v[q] = 0.f;
+			if (W) {
+				ld8(W + i, t);
+#pragma unroll
+				for (int q = 0; q < 8; q++) v[q] = alpha * t[q];
+			}
+			if (E) {
+				ld8(E + i, t);
+#pragma unroll
+				for (int q = 0; q < 8; q++) v[q] -= ac0 * t[q];
+			}
+			if (P) {
+				ld8(P + i, t);
+#pragma unroll
+				for (int q = 0; q < 8; q++) v[q] -= beta * t[q];
+			}
+			if (R) {
+				ld8(R + i, t);
+#pragma unroll
+				for (int q = 0; q < 8; q++) v[q] += cf.r[col + q] * t[q];
+			}
+			if (X) {
+				ld8(X + i, t);
+#pragma unroll
+				for (int q = 0; q < 8; q++) v[q] += cf.x[col + q] * t[q];
+			}
+			st8(O + i, v);
+		}
+		return;
+	}
 	if ((b & 3) == 0) {
 		// four consecutive elements of one row per thread
 		for (int64_t i4 = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i4 < count / 4; i4 += tstride) {
