@@ -52,7 +52,10 @@ namespace eig {
 
 constexpr int kMaxB = 64;
 constexpr int kThreads = 256;
-constexpr int kMixedMaxDegree = 8;
+#ifndef FMX_MIXED_MAX_DEGREE
+#define FMX_MIXED_MAX_DEGREE 8
+#endif
+constexpr int kMixedMaxDegree = FMX_MIXED_MAX_DEGREE;
 
 #define ECUDA_TRY(call)                                                         \
 	do {                                                                        \

@@ -21,8 +21,8 @@ namespace fmx {
 constexpr uint32_t kExactMax = FMX_EXACT_ROW_MAX;  // rows summed by one lane group
 constexpr uint32_t kChunk = 256;        // most entries per chunk of a longer row
 #ifndef FMX_RANGE_ENTRIES
-#define FMX_RANGE_ENTRIES 128           // measured at R-MAT scale 24, k = 16: 1.96 ms per call against
-                                        // 1.99-2.01 ms for 256 (more, evener ranges for the grid)
+#define FMX_RANGE_ENTRIES 256           // 128 measured within 1 % at R-MAT scale 24, k = 16, but 15 %
+                                        // slower for k = 1 (a warp per range) and 5 % at scale 26
 #endif
 constexpr uint32_t kRange = FMX_RANGE_ENTRIES;  // target entries per multi-row range
 constexpr uint32_t kLongChunks = 8;     // heavy rows with more chunks get a warp each in the fixup
