@@ -24,7 +24,19 @@ constexpr uint32_t kChunk = 256;        // most entries per chunk of a longer ro
 #define FMX_RANGE_ENTRIES 256           // 128 measured within 1 % at R-MAT scale 24, k = 16, but 15 %
                                         // slower for k = 1 (a warp per range) and 5 % at scale 26
 #endif
-constexpr uint32_t kRange = FMX_RANGE_ENTRIES;  // target entries per multi-row range
+constexpr uint32_t kRange = FMX_RANGE_ENTRIES;  // most target entries per multi-row range
+#ifndef FMX_RANGE_MIN
+#define FMX_RANGE_MIN 128               // 32 or 64 took SBM eigensolves (n 10k-200k) 5-15 % further,
+                                        // but slowed PageRank at R-MAT scale 16 (k = 1) by 9-23 %
+#endif
+#ifndef FMX_RANGE_FILL_PER_GROUP
+#define FMX_RANGE_FILL_PER_GROUP 1
+#endif
+constexpr uint32_t kRangeMin = FMX_RANGE_MIN;   // fewest: small matrices get shorter runs, so that they
+                                                // still fill the grid
+// lane groups of a full grid at k = 16 (148 SMs x 32 warps x 16 groups)
+// times the runs each should get before runs shrink below kRange
+constexpr uint64_t kRangeFill = uint64_t(FMX_RANGE_FILL_PER_GROUP) * 148 * 32 * 16;
 constexpr uint32_t kLongChunks = 8;     // heavy rows with more chunks get a warp each in the fixup
 constexpr uint32_t kBlockChunks = 64;   // heavy rows with more chunks get a block of 8 warps each
 #ifndef FMX_HOT_MAX
@@ -137,12 +149,24 @@ namespace fmx {
 // The work segments' rule, shared by both schedulers: rows are taken in
 // order with `len` = their entry count (1..kExactMax) or 1 (an empty or
 // longer row: one zero-row entry); row r opens a new run when the running
-// total of the lens before it, L[r], enters a new multiple of kRange
-// (L[r] / kRange differs from L[r-1] / kRange).  A run therefore holds at
-// most kRange - 1 + kExactMax entries.  A row longer than kExactMax also
-// gets ceil(d / kChunk) equal chunks, chunk c holding entries
+// total of the lens before it, L[r], enters a new multiple of the run size
+// R = range_entries(L[n]) (L[r] / R differs from L[r-1] / R).  A run
+// therefore holds at most kRange - 1 + kExactMax entries.  A row longer than
+// kExactMax also gets ceil(d / kChunk) equal chunks, chunk c holding entries
 // [d c / cnt, d (c + 1) / cnt).
 __host__ __device__ inline uint32_t seg_row_len(uint32_t d) { return (d >= 1 && d <= kExactMax) ? d : 1; }
+
+// Run size for rows whose lens add up to `total`: kRange, or less (down to
+// kRangeMin, a multiple of kStep) when that would leave fewer than
+// kRangeFill runs, so that small matrices still spread over the grid.
+// Measured on 40 held-out SBM graphs (n 10k-200k, about 2M entries, runs of
+// 128 instead of 256): plain eigensolves 4.8 -> 3.6 ms median.
+__host__ __device__ inline uint32_t range_entries(uint64_t total)
+{
+	uint64_t r = total / kRangeFill;
+	r = r < kRangeMin ? kRangeMin : (r > kRange ? kRange : r);
+	return uint32_t(r / kStep * kStep);
+}
 
 // Device-resident CSR (rows ascending, columns in entry order); the
 // pointers are owned by `own` and released on `st` when it is destroyed.

@@ -10,8 +10,8 @@
 //   2. per row: len = seg_row_len(d), chunk count, heavy flag; exclusive
 //      scans give the lens before each row (L), the first chunk of each
 //      heavy row and its heavy index
-//   3. run segments: row r opens one when L[r] / kRange differs from
-//      L[r - 1] / kRange (the rule in part.h); chunk segments follow in
+//   3. run segments: row r opens one when L[r] / R differs from L[r - 1] / R,
+//      R = range_entries(L[n]) (the rule in part.h); chunk segments follow in
 //      heavy-row order; padded lengths, scanned into stream offsets
 //   4. ranges: the stable radix sort of the segments by padded length,
 //      longest first
@@ -101,10 +101,10 @@ __global__ void row_info_kernel(const uint32_t *row_ptr, uint64_t n, uint64_t *l
 	if ((threadIdx.x & 31) == 0 && ex) atomicAdd(n_exact, ex);
 }
 
-// start[r] = 1 when row r opens a run (index n holds 0)
-__global__ void start_kernel(const uint64_t *L, uint64_t n, uint32_t *start)
+// start[r] = 1 when row r opens a run of `run` entries (index n holds 0)
+__global__ void start_kernel(const uint64_t *L, uint64_t n, uint32_t run, uint32_t *start)
 {
-	GRID_STRIDE(r, n + 1) start[r] = r < n && (r == 0 || L[r] / kRange != L[r - 1] / kRange);
+	GRID_STRIDE(r, n + 1) start[r] = r < n && (r == 0 || L[r] / run != L[r - 1] / run);
 }
 
 // run segment s = sidx[r] of a row r that opens one: first row, lens before it
@@ -356,7 +356,9 @@ int make_part_device(const dev_csr &csr, int device, cudaStream_t st, std::share
 	TRY(excl_scan(t, lens, L, n + 1));
 	TRY(excl_scan(t, chunks, cfirst, n + 1));
 	TRY(excl_scan(t, hflag, hidx, n + 1));
-	start_kernel<<<grid(n + 1), kT, 0, st>>>(L, n, start);
+	uint64_t total_len = 0;
+	TRY(fetch(L + n, total_len, st));
+	start_kernel<<<grid(n + 1), kT, 0, st>>>(L, n, range_entries(total_len), start);
 	SCUDA_TRY(cudaGetLastError());
 	TRY(excl_scan(t, start, sidx, n + 1));
 	uint32_t s_run = 0, n_chunks = 0, n_heavy = 0;

@@ -19,7 +19,7 @@
 //                               entry slot s + 1 names hot_col[s], slot 0 the
 //                               pack's zero row
 //   ranges   range_t[]          work units, sorted by entry count (largest
-//                               first): a run of consecutive rows of ~kRange
+//                               first): a run of consecutive rows of up to ~kRange
 //                               entries, or one of the equal chunks (<= kChunk
 //                               entries) of a longer row.  Each starts at a
 //                               multiple of 8 entries and is padded to one
@@ -1106,14 +1106,17 @@ static int make_part(const host_csr &csr, int device, std::shared_ptr<gpu_part> 
 	std::vector<heavy_row> heavy;
 	uint32_t n_exact = 0;
 	{
+		uint64_t total = 0;
+		for (uint64_t r = 0; r < n; r++) total += seg_row_len(csr.row_ptr[r + 1] - csr.row_ptr[r]);
+		const uint32_t run = range_entries(total);
 		uint64_t L = 0, bucket = ~0ull;           // lens of the rows before r
 		for (uint64_t r = 0; r < n; r++) {
 			const uint32_t d = csr.row_ptr[r + 1] - csr.row_ptr[r];
 			const uint32_t len = seg_row_len(d);
 			n_exact += (d >= 1 && d <= kExactMax);
-			if (L / kRange != bucket) {
+			if (L / run != bucket) {
 				segs.push_back({r, r + 1, 0, 0, kNoSlot, 0, 0});
-				bucket = L / kRange;
+				bucket = L / run;
 			} else {
 				segs.back().row1 = r + 1;
 			}
