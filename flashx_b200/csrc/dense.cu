@@ -120,15 +120,30 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16])
 // Shared-memory matrix descriptor, no swizzle (canonical "interleave"
 // layout of 8-row x 16-byte core matrices): start, leading and stride byte
 // offsets in 16-byte units, version 1 (sm100).
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo_bytes, uint32_t sbo_bytes)
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo_bytes, uint32_t sbo_bytes,
+		uint32_t layout = 0)
 {
 	uint64_t d = 0;
 	d |= uint64_t((addr >> 4) & 0x3FFF);
 	d |= uint64_t((lbo_bytes >> 4) & 0x3FFF) << 16;
 	d |= uint64_t((sbo_bytes >> 4) & 0x3FFF) << 32;
 	d |= uint64_t(1) << 46;                  // version
-	return d;                                // base offset 0, layout SWIZZLE_NONE (0)
+	d |= uint64_t(layout & 7) << 61;         // 0: no swizzle; 1: 128-byte swizzle of 32-byte atoms
+	return d;                                // base offset 0
 }
+// The 128-byte swizzle of 32-byte atoms (layout type 1), the one MN-major
+// form TF32 operands take (unswizzled MN-major TF32 products came out zero):
+// an operand is blocks of 32 elements along M (N), each holding a tile's K
+// rows as 128-byte rows, 4 rows to a 512-byte atom, the 32-byte chunk index
+// XORed with the row's index in its atom.  Byte offset of element e (along M
+// or N) of K row r:
+__host__ __device__ constexpr uint32_t sw32_offset(int e, int r)
+{
+	return uint32_t(e / 32) * 16384u + uint32_t(r / 4) * 512u + uint32_t(r % 4) * 128u +
+			uint32_t(((e % 32) / 8) ^ (r % 4)) * 32u + uint32_t(e % 8) * 4u;
+}
+constexpr uint32_t kSw32Block = 16384;   // bytes of one 32-element block of a 128-row tile
+constexpr uint32_t kSw32Atom = 512;      // bytes of 4 K rows
 // Instruction descriptor: FP32 accumulate, A/B format (1 = BF16, 2 = TF32),
 // majors (0 = K-major, 1 = MN-major), N, M = 128.
 __host__ __device__ constexpr uint32_t instr_desc(uint32_t fmt, uint32_t a_mn, uint32_t b_mn, uint32_t n)
@@ -1112,6 +1127,7 @@ __global__ void chol_inv_kernel(const double *__restrict__ G, int b, double *__r
 // threads (disjoint pairs touch disjoint rows and columns), the off-diagonal
 // norm is a CTA reduction, and the final order is a parallel rank count.
 constexpr int kJacobiThreads = 256;
+constexpr double kJacobiOff2 = 1e-24;    // stop when sum of squared off-diagonals / diagonal's is below
 
 __global__ void __launch_bounds__(kJacobiThreads) jacobi_eig_kernel(const double *__restrict__ H, int b,
 		double *__restrict__ w, double *__restrict__ V, int max_sweeps)
@@ -1153,7 +1169,7 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_eig_kernel(const double
 			off = a / (d > 0 ? d : 1.0);
 		}
 		__syncthreads();
-		if (off < 1e-30) break;
+		if (off < kJacobiOff2) break;
 		for (int step = 0; step < m - 1; step++) {
 			// round-robin tournament pairing of 0..m-1
 			if (t < half) {
@@ -1278,7 +1294,10 @@ __global__ void __launch_bounds__(kJacobiSmallThreads) jacobi_small_kernel(const
 		__syncthreads();
 		so = 0; sd = 0;
 		for (int i = 0; i < NW; i++) { so += red[0][i]; sd += red[1][i]; }
-		if (so / (sd > 0 ? sd : 1.0) < 1e-30) break;    // the same decision in every thread
+		// the same decision in every thread: off-diagonal norm below 1e-12 of
+		// the diagonal's (squared 1e-24), far below what the 1e-6 residuals
+		// of the solve need; a sweep more (to 1e-30) cost about 14 %
+		if (so / (sd > 0 ? sd : 1.0) < kJacobiOff2) break;
 		for (int step = 0; step < m - 1; step++) {
 			const double (*A)[kJacobiSmallMax + 1] = Ab[cur];
 			const double (*Q)[kJacobiSmallMax + 1] = Qb[cur];
@@ -1342,6 +1361,160 @@ __global__ void __launch_bounds__(kJacobiSmallThreads) jacobi_small_kernel(const
 	__syncthreads();
 	for (int i = t; i < b; i += NT) w[i] = A[order[i]][order[i]];
 	for (int i = t; i < b * b; i += NT) V[i] = Q[i / b][order[i % b]];
+}
+
+// ---------------------------------------------------------------------------
+// G = X^T W in 3xTF32 for 16-column blocks stored back to back (the
+// eigensolver's b = 16), on MN-major operands in the swizzled 32-byte-atom
+// layout (sw32_offset).  A 128-row tile is two 16 KB blocks, one per side;
+// block row r holds
+//   elements 0-15   the row's 16 FP32 values, copied from global memory by
+//                   cp.async straight into place: the MMA reads them as
+//                   TF32, so they are the hi parts (x with its low 13
+//                   mantissa bits dropped)
+//   elements 16-31  the lo parts x - hi, written by the converters
+// so the converters write 4 bytes per element instead of 8, and no
+// transpose.  One MMA per 8 rows: A = the X block (M = 64; rows 32-63 read
+// the W block that follows and are never read out), B = the W block (N =
+// 32), so D holds [hi*hi | hi*lo] over [lo*hi | lo*lo].  Converter groups of
+// 4 warps (a thread per tile row) own rings of kX3Stages stages; group g
+// takes the CTA's tiles g, g + kX3Groups, ...; one thread of warp 0 issues
+// the MMAs; every wait is bounded.  Two partials per CTA (rows of hi parts:
+// hi*hi + hi*lo; rows of lo parts: lo*hi), reduced by gram_reduce_kernel.
+// ---------------------------------------------------------------------------
+constexpr int kX3Groups = 2, kX3Stages = 3;
+constexpr uint32_t kX3Stage = 2 * kSw32Block;   // X block + W block
+constexpr int kX3Threads = 32 * (1 + 4 * kX3Groups);
+constexpr size_t kX3Smem = size_t(kX3Groups) * kX3Stages * kX3Stage;
+
+__global__ void __launch_bounds__(kX3Threads, 1)
+tc_gram_x3s_kernel(const float *__restrict__ X, const float *__restrict__ W, int64_t n, float *__restrict__ part,
+		int *err)
+{
+	extern __shared__ __align__(1024) char smem[];
+	__shared__ uint64_t full[kX3Groups * kX3Stages], empty[kX3Groups * kX3Stages], accf;
+	__shared__ uint32_t tmem_base;
+	__shared__ int bad;
+	constexpr uint32_t ncols = 32;
+	const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+	if (warp == 0) tmem_alloc(&tmem_base, ncols);
+	if (tid == 0) {
+		for (int i = 0; i < kX3Groups * kX3Stages; i++) { mbar_init(&full[i], 4); mbar_init(&empty[i], 1); }
+		mbar_init(&accf, 1);
+		bad = 0;
+		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+	}
+	tc_fence_before();
+	__syncthreads();
+	tc_fence_after();
+	const uint32_t tmem = tmem_base;
+	const int64_t ntiles = (n + kTile - 1) / kTile;
+	const int64_t my_tiles = int64_t(blockIdx.x) < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+	auto tile_row = [&](int64_t i) { return (int64_t(blockIdx.x) + i * int64_t(gridDim.x)) * kTile; };
+	// tile i: group i % G, its (i / G)-th tile, stage (i / G) % S of that group
+	auto stage_of = [&](int64_t i) { return int((i % kX3Groups) * kX3Stages + (i / kX3Groups) % kX3Stages); };
+	auto use_of = [&](int64_t i) { return uint32_t((i / kX3Groups) / kX3Stages); };
+	bool ok = true;
+	if (warp == 0) {
+		if (lane == 0) {
+			const uint32_t idesc = instr_desc_m64(2, 1, 1, 32);
+			for (int64_t i = 0; i < my_tiles && ok; i++) {
+				const int s = stage_of(i);
+				if (!mbar_wait(&full[s], use_of(i) & 1)) { ok = false; break; }
+				tc_fence_after();
+				const uint32_t base = smem_u32(smem + size_t(s) * kX3Stage);
+				uint64_t a = smem_desc(base, kSw32Block, kSw32Atom, 1);
+				uint64_t b = smem_desc(base + kSw32Block, kSw32Block, kSw32Atom, 1);
+				for (int ks = 0; ks < kTile / 8; ks++) {        // 8 K rows = 2 atoms per MMA
+					umma<true>(tmem, a, b, idesc, (i > 0 || ks > 0) ? 1u : 0u);
+					a += 2 * kSw32Atom / 16;
+					b += 2 * kSw32Atom / 16;
+				}
+				umma_commit(&empty[s]);
+			}
+			umma_commit(&accf);
+		}
+	} else {
+		const int g = (warp - 1) / 4;
+		const int r = tid - 32 - 128 * g;                  // the thread's tile row
+		const int h = (r >> 2) & 1;                        // 16-byte half taken first: a warp's 16-byte
+		                                                   // accesses then cover all 32 banks
+		// local tile j of the group: the CTA's tile g + j G
+		auto issue = [&](int64_t j) {
+			const int64_t i = g + j * kX3Groups;
+			if (i < my_tiles && ok) {
+				const int s = stage_of(i);
+				// the stage's previous tile must be through the MMA
+				if (i >= int64_t(kX3Groups) * kX3Stages && !mbar_wait(&empty[s], (use_of(i) - 1) & 1)) ok = false;
+				const int64_t row = tile_row(i) + r;
+				if (ok && row < n) {
+					char *xb = smem + size_t(s) * kX3Stage;
+					const float *sx = X + row * 16, *sw = W + row * 16;
+#pragma unroll
+					for (int q = 0; q < 4; q++) {
+						const int u = q ^ h;
+						cp_async16(xb + sw32_offset(4 * u, r), sx + 4 * u);
+						cp_async16(xb + kSw32Block + sw32_offset(4 * u, r), sw + 4 * u);
+					}
+				}
+			}
+			cp_async_commit();                            // one group per tile (empty past the end)
+		};
+		for (int j = 0; j < kX3Stages - 1; j++) issue(j);
+		for (int64_t j = 0, i = g; i < my_tiles && ok; j++, i += kX3Groups) {
+			issue(j + kX3Stages - 1);
+			cp_async_wait<kX3Stages - 1>();                // this thread's copies of tile i have landed
+			ok = __all_sync(0xffffffffu, ok);              // warp-uniform exit (the __syncwarp below)
+			if (!ok) break;
+			const int s = stage_of(i);
+			const bool live = tile_row(i) + r < n;
+			for (int side = 0; side < 2; side++) {
+				char *blk = smem + size_t(s) * kX3Stage + side * kSw32Block;
+#pragma unroll
+				for (int q = 0; q < 4; q++) {
+					const int u = q ^ h;
+					uint4 v = live ? *reinterpret_cast<const uint4 *>(blk + sw32_offset(4 * u, r)) : make_uint4(0, 0, 0, 0);
+					if (!live) *reinterpret_cast<uint4 *>(blk + sw32_offset(4 * u, r)) = v;   // a row past n adds zeros
+					const uint32_t x[4] = {v.x, v.y, v.z, v.w};
+					uint32_t lo[4];
+#pragma unroll
+					for (int e = 0; e < 4; e++)
+						lo[e] = __float_as_uint(__fsub_rn(__uint_as_float(x[e]), __uint_as_float(x[e] & 0xFFFFE000u)));
+					*reinterpret_cast<uint4 *>(blk + sw32_offset(16 + 4 * u, r)) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+				}
+			}
+			fence_async_smem();                            // cp.async data and lo parts -> the MMA
+			__syncwarp();
+			if (lane == 0) mbar_arrive(&full[s]);
+		}
+		cp_async_wait<0>();                                // no copy in flight when the CTA exits
+		if (g == 0) {
+			// warp quarter q holds D rows 16 q .. 16 q + 15 in lanes 32 q .. 32 q + 15
+			const bool done = ok && mbar_wait(&accf, 0);
+			const bool all = __all_sync(0xffffffffu, done);
+			ok = ok && done;
+			if (all) {
+				tc_fence_after();
+				const int q = warp & 3;
+				const int dm = 16 * q + lane;
+				const bool hi_row = dm < 16;
+				const int m = hi_row ? dm : dm - 16;
+				float o[16], o2[16];
+				tmem_ld16(tmem + (uint32_t(q * 32) << 16), o);
+				tmem_ld16(tmem + (uint32_t(q * 32) << 16) + 16u, o2);
+				if (lane < 16 && m < 16) {
+					float *pp = part + (size_t(2 * blockIdx.x) + (hi_row ? 0 : 1)) * 256 + size_t(m) * 16;
+					for (int c = 0; c < 16; c++) pp[c] = my_tiles ? (hi_row ? __fadd_rn(o[c], o2[c]) : o[c]) : 0.f;
+				}
+			}
+		}
+	}
+	if (!ok) atomicExch(&bad, 1);
+	tc_fence_before();
+	__syncthreads();
+	tc_fence_after();
+	if (tid == 0 && bad) atomicExch(err, 1);
+	if (warp == 0) tmem_dealloc(tmem, ncols);
 }
 
 int sms(int device)
@@ -1439,6 +1612,17 @@ int fmx_dense_gram(int precision, const float *X, int64_t ldx, int M, const floa
 	if (!err) return set_error(FMX_ERR_INVAL, "null error flag");
 	const bool tf32 = precision == FMX_DENSE_TF32X3;
 	if (!tf32 && precision != FMX_DENSE_BF16) return set_error(FMX_ERR_INVAL, "unknown precision %d", precision);
+	if (tf32 && M == 16 && N == 16 && ldx == 16 && ldw == 16 && (reinterpret_cast<uintptr_t>(X) & 15) == 0 &&
+			(reinterpret_cast<uintptr_t>(W) & 15) == 0 && n > 0) {
+		// 16-column blocks back to back: hi parts copied into place, one pass
+		DCUDA_TRY(cudaFuncSetAttribute(tc_gram_x3s_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kX3Smem)));
+		tc_gram_x3s_kernel<<<parts / 2, kX3Threads, kX3Smem, st>>>(X, W, n, static_cast<float *>(part), err);
+		DCUDA_TRY(cudaGetLastError());
+		gram_reduce_kernel<float><<<(M * N + 7) / 8, 256, 0, st>>>(static_cast<const float *>(part), parts, M * N,
+				static_cast<float *>(G));
+		DCUDA_TRY(cudaGetLastError());
+		return FMX_OK;
+	}
 	if (ldx % 4 == 0 && ldw % 4 == 0 && ldx <= 64 && ldw <= 64 && (reinterpret_cast<uintptr_t>(X) & 15) == 0 &&
 			(reinterpret_cast<uintptr_t>(W) & 15) == 0 && n > 0 && (!tf32 || M <= 32)) {
 		const pipe_plan P4(true, tf32, M, N, ldx, ldw, 3, 4), P2(true, tf32, M, N, ldx, ldw, 3, 2),

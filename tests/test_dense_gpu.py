@@ -47,7 +47,7 @@ def test_tc_gemm(torch_cuda, prec, n, K, N, ldx):
 
 
 @pytest.mark.parametrize("prec", [_lib.DENSE_BF16, _lib.DENSE_TF32X3, _lib.DENSE_F64])
-@pytest.mark.parametrize("n,M,N", [(1000, 16, 16), (200001, 16, 16), (65536, 32, 32), (4097, 48, 16), (129, 64, 64),
+@pytest.mark.parametrize("n,M,N", [(1000, 16, 16), (200001, 16, 16), (100, 16, 16), (65536, 32, 32), (4097, 48, 16), (129, 64, 64),
                                    (50, 16, 48), (777, 12, 5), (3, 1, 16), (99999, 8, 8), (100003, 16, 9)])
 def test_gram(torch_cuda, prec, n, M, N):
     _gram_case(torch_cuda, prec, n, M, N, M, N)
