@@ -13,6 +13,9 @@
 //       BF16   one MMA per K step, FP32 accumulate (early, loose iterations)
 //       TF32x3 x = hi + lo split (hi = tf32(x), lo = tf32(x - hi)); the
 //              products hi*hi + hi*lo + lo*hi reach FP32 accuracy
+//     For 16-column blocks stored back to back the 3xTF32 forms copy X rows
+//     into place as the hi parts (tc_gemm_x3s, tc_gram_x3s), since the MMA
+//     reads FP32 as TF32 by dropping the low mantissa bits.
 //  gram_f64  G = X^T W in FP64 on the CUDA cores (Cholesky-QR, residuals)
 //  small FP64 kernels on one CTA: Cholesky factor inverse, Jacobi
 //  eigendecomposition (the projected Rayleigh-Ritz problem).
@@ -359,6 +362,25 @@ tc_gemm_kernel(const float *__restrict__ X, int64_t ldx, int K, const float *__r
 //     so the threads' 4-byte stores hit 32 banks; A's 64 rows per K unit
 //     overlap the next unit's rows, which only feeds unread D rows.
 // ---------------------------------------------------------------------------
+// Raw tiles in flight per converter thread and converter groups (when they
+// fit), measured at n = 4.2M, 16 columns.  GEMM: 3 and 4 (BF16 144 us; 1 and
+// 6: 156 us).  Gram: 1 and 6 (BF16 162 us; 3 and 4: 203 us, 2 and 4: 175 us):
+// the Gram's raw rows are twice as wide, and more groups in flight beat a
+// deeper ring per group.
+#ifndef FMX_PIPE_GEMM_RS
+#define FMX_PIPE_GEMM_RS 3
+#endif
+#ifndef FMX_PIPE_GEMM_NG
+#define FMX_PIPE_GEMM_NG 4
+#endif
+#ifndef FMX_PIPE_GRAM_RS
+#define FMX_PIPE_GRAM_RS 1
+#endif
+#ifndef FMX_PIPE_GRAM_NG
+#define FMX_PIPE_GRAM_NG 6
+#endif
+constexpr int kGemmRS = FMX_PIPE_GEMM_RS, kGemmNG = FMX_PIPE_GEMM_NG;
+constexpr int kGramRS = FMX_PIPE_GRAM_RS, kGramNG = FMX_PIPE_GRAM_NG;
 constexpr size_t kPipeSmemBudget = size_t(200) << 10;   // the rings' target size
 constexpr size_t kPipeSmemMax = size_t(220) << 10;      // at most (227 KB per CTA, less the static part)
 
@@ -1382,7 +1404,15 @@ __global__ void __launch_bounds__(kJacobiSmallThreads) jacobi_small_kernel(const
 // the MMAs; every wait is bounded.  Two partials per CTA (rows of hi parts:
 // hi*hi + hi*lo; rows of lo parts: lo*hi), reduced by gram_reduce_kernel.
 // ---------------------------------------------------------------------------
-constexpr int kX3Groups = 2, kX3Stages = 3;
+// 6 groups of 1 stage: measured at n = 4.2M, 165 us; 4 x 1 183, 3 x 2 181,
+// 2 x 3 224 us (more tiles in flight per CTA, no deeper ring per group)
+#ifndef FMX_X3_GROUPS
+#define FMX_X3_GROUPS 6
+#endif
+#ifndef FMX_X3_STAGES
+#define FMX_X3_STAGES 1
+#endif
+constexpr int kX3Groups = FMX_X3_GROUPS, kX3Stages = FMX_X3_STAGES;
 constexpr uint32_t kX3Stage = 2 * kSw32Block;   // X block + W block
 constexpr int kX3Threads = 32 * (1 + 4 * kX3Groups);
 constexpr size_t kX3Smem = size_t(kX3Groups) * kX3Stages * kX3Stage;
@@ -1517,6 +1547,173 @@ tc_gram_x3s_kernel(const float *__restrict__ X, const float *__restrict__ W, int
 	if (warp == 0) tmem_dealloc(tmem, ncols);
 }
 
+// ---------------------------------------------------------------------------
+// Y = X B in 3xTF32 for 16 x 16 B and 16-column X and Y stored back to back
+// (the eigensolver's basis updates at b = 16).  A = the X tile, K-major in
+// the no-swizzle layout (16-byte unit u of row r at u 2048 + r 16): each
+// row's 4 units are copied by cp.async straight into place, where the MMA
+// reads them as TF32, their hi parts; the converters write only the lo parts
+// x - hi into a second such tile.  B^T hi and lo (B split by rounding) sit
+// in shared memory for the whole kernel.  Per tile, three MMA passes of two
+// K steps (hi B_hi, hi B_lo, lo B_hi) into one of kGx3Acc TMEM accumulators,
+// which 4 epilogue warps drain into Y while the next tiles run.  Converter
+// groups of 4 warps own rings of kGx3Stages stages; every wait is bounded.
+// ---------------------------------------------------------------------------
+// 4 groups of 2 stages: measured at n = 4.2M, 139 us; 3 x 2 140, 3 x 3 144,
+// 2 x 4 171, 2 x 6 182 us (more stages in flight per group are slower)
+#ifndef FMX_GX3_GROUPS
+#define FMX_GX3_GROUPS 4
+#endif
+#ifndef FMX_GX3_STAGES
+#define FMX_GX3_STAGES 2
+#endif
+constexpr int kGx3Groups = FMX_GX3_GROUPS, kGx3Stages = FMX_GX3_STAGES, kGx3Acc = 8;
+constexpr uint32_t kGx3Part = 4u * kTile * 16;   // one 128 x 16 FP32 tile (4 units)
+constexpr uint32_t kGx3Stage = 2 * kGx3Part;      // hi (copied) + lo
+constexpr uint32_t kGx3BPart = 4u * 16 * 16;      // B^T (16 x 16) in 4 units
+constexpr int kGx3Threads = 32 * (1 + 4 * kGx3Groups + 4);
+constexpr size_t kGx3Smem = size_t(kGx3Groups) * kGx3Stages * kGx3Stage + 2 * kGx3BPart;
+
+__global__ void __launch_bounds__(kGx3Threads, 1)
+tc_gemm_x3s_kernel(const float *__restrict__ X, const float *__restrict__ B, int ldb, float *__restrict__ Y,
+		int64_t n, int *err)
+{
+	extern __shared__ __align__(1024) char smem[];
+	__shared__ uint64_t full[kGx3Groups * kGx3Stages], empty[kGx3Groups * kGx3Stages], accf[kGx3Acc], acce[kGx3Acc];
+	__shared__ uint32_t tmem_base;
+	__shared__ int bad;
+	constexpr uint32_t ncols = 16 * kGx3Acc;
+	constexpr int kEpi0 = 1 + 4 * kGx3Groups;          // first epilogue warp
+	const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+	char *sb = smem + size_t(kGx3Groups) * kGx3Stages * kGx3Stage;   // B^T hi, then lo
+	for (int j = tid; j < 16; j += blockDim.x) {
+		float col[16];
+		for (int k = 0; k < 16; k++) col[k] = B[size_t(k) * ldb + j];
+		for (int pt = 0; pt < 2; pt++) put_units<true>(sb + pt * kGx3BPart, 16 * 16, j, col, 16, 16, pt);
+	}
+	if (warp == 0) tmem_alloc(&tmem_base, ncols);
+	if (tid == 0) {
+		for (int i = 0; i < kGx3Groups * kGx3Stages; i++) { mbar_init(&full[i], 4); mbar_init(&empty[i], 1); }
+		for (int i = 0; i < kGx3Acc; i++) { mbar_init(&accf[i], 1); mbar_init(&acce[i], 4); }
+		bad = 0;
+		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+	}
+	fence_async_smem();                                 // B^T -> the MMA
+	tc_fence_before();
+	__syncthreads();
+	tc_fence_after();
+	const uint32_t tmem = tmem_base;
+	const int64_t ntiles = (n + kTile - 1) / kTile;
+	const int64_t my_tiles = int64_t(blockIdx.x) < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+	auto tile_row = [&](int64_t i) { return (int64_t(blockIdx.x) + i * int64_t(gridDim.x)) * kTile; };
+	auto stage_of = [&](int64_t i) { return int((i % kGx3Groups) * kGx3Stages + (i / kGx3Groups) % kGx3Stages); };
+	auto use_of = [&](int64_t i) { return uint32_t((i / kGx3Groups) / kGx3Stages); };
+	bool ok = true;
+	if (warp == 0) {
+		if (lane == 0) {
+			const uint32_t idesc = instr_desc(2, 0, 0, 16);
+			const uint64_t dB = smem_desc(smem_u32(sb), 16 * 16, 128);
+			int64_t issued = 0;
+			for (int64_t i = 0; i < my_tiles && ok; i++) {
+				const int s = stage_of(i), b = int(i % kGx3Acc);
+				if (i >= kGx3Acc && !mbar_wait(&acce[b], uint32_t((i / kGx3Acc - 1) & 1))) { ok = false; break; }
+				if (!mbar_wait(&full[s], use_of(i) & 1)) { ok = false; break; }
+				tc_fence_after();
+				const uint64_t dHi = smem_desc(smem_u32(smem + size_t(s) * kGx3Stage), kTile * 16, 128);
+				const uint32_t d = tmem + uint32_t(b * 16);
+				uint32_t acc = 0;
+				for (int pass = 0; pass < 3; pass++) {
+					// (hi, B hi), (hi, B lo), (lo, B hi)
+					uint64_t a = dHi + (pass == 2 ? kGx3Part / 16 : 0);
+					uint64_t bd = dB + (pass == 1 ? kGx3BPart / 16 : 0);
+					for (int ks = 0; ks < 2; ks++) {            // 16 K = two MMAs of 8
+						umma<true>(d, a, bd, idesc, acc);
+						acc = 1;
+						a += 2 * kTile * 16 / 16;
+						bd += 2 * 16 * 16 / 16;
+					}
+				}
+				umma_commit(&empty[s]);
+				umma_commit(&accf[b]);
+				issued = i + 1;
+			}
+			// the MMAs issued must be complete before TMEM is released
+			if (issued && !mbar_wait(&accf[(issued - 1) % kGx3Acc], uint32_t(((issued - 1) / kGx3Acc) & 1))) ok = false;
+		}
+	} else if (warp < kEpi0) {
+		const int g = (warp - 1) / 4;
+		const int r = tid - 32 - 128 * g;                  // the thread's tile row
+		auto issue = [&](int64_t j) {
+			const int64_t i = g + j * kGx3Groups;
+			if (i < my_tiles && ok) {
+				const int s = stage_of(i);
+				if (i >= int64_t(kGx3Groups) * kGx3Stages && !mbar_wait(&empty[s], (use_of(i) - 1) & 1)) ok = false;
+				const int64_t row = tile_row(i) + r;
+				if (ok && row < n) {
+					char *hb = smem + size_t(s) * kGx3Stage;
+					const float *sx = X + row * 16;
+#pragma unroll
+					for (int u = 0; u < 4; u++) cp_async16(hb + size_t(u) * kTile * 16 + size_t(r) * 16, sx + 4 * u);
+				}
+			}
+			cp_async_commit();                            // one group per tile (empty past the end)
+		};
+		for (int j = 0; j < kGx3Stages - 1; j++) issue(j);
+		for (int64_t j = 0, i = g; i < my_tiles && ok; j++, i += kGx3Groups) {
+			issue(j + kGx3Stages - 1);
+			cp_async_wait<kGx3Stages - 1>();               // this thread's copies of tile i have landed
+			ok = __all_sync(0xffffffffu, ok);              // warp-uniform exit (the __syncwarp below)
+			if (!ok) break;
+			const int s = stage_of(i);
+			char *hb = smem + size_t(s) * kGx3Stage;
+			const bool live = tile_row(i) + r < n;
+#pragma unroll
+			for (int u = 0; u < 4; u++) {
+				char *ph = hb + size_t(u) * kTile * 16 + size_t(r) * 16;
+				uint4 v = live ? *reinterpret_cast<const uint4 *>(ph) : make_uint4(0, 0, 0, 0);
+				if (!live) *reinterpret_cast<uint4 *>(ph) = v;   // a row past n adds zeros
+				const uint32_t x[4] = {v.x, v.y, v.z, v.w};
+				uint32_t lo[4];
+#pragma unroll
+				for (int e = 0; e < 4; e++)
+					lo[e] = __float_as_uint(__fsub_rn(__uint_as_float(x[e]), __uint_as_float(x[e] & 0xFFFFE000u)));
+				*reinterpret_cast<uint4 *>(ph + kGx3Part) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+			}
+			fence_async_smem();                            // cp.async data and lo parts -> the MMA
+			__syncwarp();
+			if (lane == 0) mbar_arrive(&full[s]);
+		}
+		cp_async_wait<0>();                                // no copy in flight when the CTA exits
+	} else {
+		// epilogue: TMEM lanes 32 q .. 32 q + 31 are tile rows
+		const int q = warp & 3;
+		for (int64_t i = 0; i < my_tiles && ok; i++) {
+			const int b = int(i % kGx3Acc);
+			const bool got = mbar_wait(&accf[b], uint32_t((i / kGx3Acc) & 1));
+			ok = __all_sync(0xffffffffu, got);
+			if (!ok) break;
+			tc_fence_after();
+			const int64_t row = tile_row(i) + q * 32 + lane;
+			float o[16];
+			tmem_ld16(tmem + (uint32_t(q * 32) << 16) + uint32_t(b * 16), o);
+			if (row < n) {
+				float4 *yr = reinterpret_cast<float4 *>(Y + row * 16);
+#pragma unroll
+				for (int v = 0; v < 4; v++) yr[v] = make_float4(o[4 * v], o[4 * v + 1], o[4 * v + 2], o[4 * v + 3]);
+			}
+			tc_fence_before();
+			__syncwarp();
+			if (lane == 0) mbar_arrive(&acce[b]);
+		}
+	}
+	if (!ok) atomicExch(&bad, 1);
+	tc_fence_before();
+	__syncthreads();
+	tc_fence_after();
+	if (tid == 0 && bad) atomicExch(err, 1);
+	if (warp == 0) tmem_dealloc(tmem, ncols);
+}
+
 int sms(int device)
 {
 	int s = 0;
@@ -1546,17 +1743,26 @@ int fmx_dense_gemm(int precision, const float *X, int64_t ldx, int64_t n, int K,
 	cudaGetDevice(&dev);
 	const int64_t tiles = (n + kTile - 1) / kTile;
 	cudaStream_t st = static_cast<cudaStream_t>(stream);
+	if (tf32 && K == 16 && N == 16 && ldx == 16 && ldy == 16 && (reinterpret_cast<uintptr_t>(X) & 15) == 0 &&
+			(reinterpret_cast<uintptr_t>(Y) & 15) == 0 && n > 0) {
+		// 16-column blocks back to back: hi parts copied into place
+		DCUDA_TRY(cudaFuncSetAttribute(tc_gemm_x3s_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kGx3Smem)));
+		const unsigned g = unsigned(std::max<int64_t>(1, std::min<int64_t>(tiles, sms(dev))));
+		tc_gemm_x3s_kernel<<<g, kGx3Threads, kGx3Smem, st>>>(X, B, ldb, Y, n, err);
+		DCUDA_TRY(cudaGetLastError());
+		return FMX_OK;
+	}
 	// the pipelined kernel when the rows of X can be bulk-copied (16-byte
 	// aligned rows of whole 16-byte units)
 	if (K % 4 == 0 && ldx % 4 == 0 && ldx <= 64 && (reinterpret_cast<uintptr_t>(X) & 15) == 0 && n > 0) {
-		// four converter groups when they fit, else two, else one
-		const pipe_plan P4(false, tf32, K, N, ldx, 0, 3, 4), P2(false, tf32, K, N, ldx, 0, 3, 2),
-				P1(false, tf32, K, N, ldx, 0, 3, 1);
+		// kGemmNG converter groups when they fit, else two, else one
+		const pipe_plan P4(false, tf32, K, N, ldx, 0, kGemmRS, kGemmNG), P2(false, tf32, K, N, ldx, 0, kGemmRS, 2),
+				P1(false, tf32, K, N, ldx, 0, kGemmRS, 1);
 		if (P4.fits() || P2.fits() || P1.fits()) {
 			const pipe_plan &P = P4.fits() ? P4 : (P2.fits() ? P2 : P1);
-			auto kern = P4.fits() ? (tf32 ? tc_pipe_kernel<true, false, 3, 4> : tc_pipe_kernel<false, false, 3, 4>)
-			          : P2.fits() ? (tf32 ? tc_pipe_kernel<true, false, 3, 2> : tc_pipe_kernel<false, false, 3, 2>)
-			                      : (tf32 ? tc_pipe_kernel<true, false, 3, 1> : tc_pipe_kernel<false, false, 3, 1>);
+			auto kern = P4.fits() ? (tf32 ? tc_pipe_kernel<true, false, kGemmRS, kGemmNG> : tc_pipe_kernel<false, false, kGemmRS, kGemmNG>)
+			          : P2.fits() ? (tf32 ? tc_pipe_kernel<true, false, kGemmRS, 2> : tc_pipe_kernel<false, false, kGemmRS, 2>)
+			                      : (tf32 ? tc_pipe_kernel<true, false, kGemmRS, 1> : tc_pipe_kernel<false, false, kGemmRS, 1>);
 			DCUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(P.smem)));
 			const unsigned grid = unsigned(std::max<int64_t>(1, std::min<int64_t>(tiles, int64_t(sms(dev)))));
 			kern<<<grid, pipe_threads(P.NG), P.smem, st>>>(X, ldx, K, nullptr, 0, N, B, ldb, Y, ldy, nullptr, n, err);
@@ -1625,14 +1831,14 @@ int fmx_dense_gram(int precision, const float *X, int64_t ldx, int M, const floa
 	}
 	if (ldx % 4 == 0 && ldw % 4 == 0 && ldx <= 64 && ldw <= 64 && (reinterpret_cast<uintptr_t>(X) & 15) == 0 &&
 			(reinterpret_cast<uintptr_t>(W) & 15) == 0 && n > 0 && (!tf32 || M <= 32)) {
-		const pipe_plan P4(true, tf32, M, N, ldx, ldw, 3, 4), P2(true, tf32, M, N, ldx, ldw, 3, 2),
-				P1(true, tf32, M, N, ldx, ldw, 3, 1);
+		const pipe_plan P4(true, tf32, M, N, ldx, ldw, kGramRS, kGramNG), P2(true, tf32, M, N, ldx, ldw, kGramRS, 2),
+				P1(true, tf32, M, N, ldx, ldw, kGramRS, 1);
 		if (P4.fits() || P2.fits() || P1.fits()) {
 			// the pipelined kernel: one CTA per SM, partials reduced in CTA order
 			const pipe_plan &P = P4.fits() ? P4 : (P2.fits() ? P2 : P1);
-			auto kern = P4.fits() ? (tf32 ? tc_pipe_kernel<true, true, 3, 4> : tc_pipe_kernel<false, true, 3, 4>)
-			          : P2.fits() ? (tf32 ? tc_pipe_kernel<true, true, 3, 2> : tc_pipe_kernel<false, true, 3, 2>)
-			                      : (tf32 ? tc_pipe_kernel<true, true, 3, 1> : tc_pipe_kernel<false, true, 3, 1>);
+			auto kern = P4.fits() ? (tf32 ? tc_pipe_kernel<true, true, kGramRS, kGramNG> : tc_pipe_kernel<false, true, kGramRS, kGramNG>)
+			          : P2.fits() ? (tf32 ? tc_pipe_kernel<true, true, kGramRS, 2> : tc_pipe_kernel<false, true, kGramRS, 2>)
+			                      : (tf32 ? tc_pipe_kernel<true, true, kGramRS, 1> : tc_pipe_kernel<false, true, kGramRS, 1>);
 			DCUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(P.smem)));
 			// the 3xTF32 kernel leaves two partials per CTA
 			kern<<<tf32 ? parts / 2 : parts, pipe_threads(P.NG), P.smem, st>>>(X, ldx, M, W, ldw, N, nullptr, 0, nullptr, 0,

@@ -22,7 +22,7 @@ def _stream(torch):
 
 
 @pytest.mark.parametrize("prec", [_lib.DENSE_BF16, _lib.DENSE_TF32X3])
-@pytest.mark.parametrize("n,K,N,ldx", [(1000, 16, 16, 16), (100003, 16, 16, 16), (50000, 32, 16, 32),
+@pytest.mark.parametrize("n,K,N,ldx", [(1000, 16, 16, 16), (100003, 16, 16, 16), (100, 16, 16, 16), (50000, 32, 16, 32),
                                        (7777, 48, 32, 48), (300, 8, 64, 8), (130, 64, 48, 64),
                                        # K padded to the MMA step; rows wider than K
                                        (999, 12, 24, 12), (4097, 20, 16, 24), (70000, 16, 16, 20),
