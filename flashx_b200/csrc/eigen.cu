@@ -779,6 +779,11 @@ struct solver {
 				ECUDA_TRY(cudaGetLastError());
 			}
 			E_TRY(fmx_dense_chol_inv(G, b, T, info + p, st));
+			// The Gram stays FP64 in both modes: the filtered block can be
+			// ill-conditioned and the Cholesky needs its accuracy.  The update
+			// runs on the tensor cores in the low-precision phase (139 us at
+			// n = 4.2M, b = 16; the FP64 row stream takes 114 us, and using it
+			// here too measured 0.2 ms faster per mixed solve at R-MAT scale 22).
 			if (tensor_cores()) {
 				f64_to_f32_kernel<<<1, 256, 0, st>>>(T, Tf, b * b);
 				ECUDA_TRY(cudaGetLastError());
@@ -798,10 +803,12 @@ struct solver {
 	int rayleigh_ritz(const float *Q)
 	{
 		E_TRY(spmm(FMX_F32, Q, b, W));
-		// The Rayleigh quotient Q^T W stays an FP64 Gram in both modes: for a
-		// block of b <= 64 columns the tensor-core Gram pads the MMA's M = 128
-		// rows with zeros (at b = 16, 7/8 of the tensor work), and measured at
-		// n = 4.2M, b = 16 it took 1.23 ms against 0.28 ms for the FP64 Gram.
+		// The Rayleigh quotient Q^T W stays an FP64 Gram in both modes.  The
+		// 3xTF32 tensor-core Gram is faster at b = 16 (165 against 263 us at
+		// n = 4.2M), but its 7e-5 relative error reaches Theta and through it
+		// the correction form's R = A X - X Theta: at R-MAT scale 22 the mixed
+		// solve then took a fifth filter pass (51 SpMMs, 66 ms, against 42 and
+		// 55 ms).
 		E_TRY(fmx_dense_gram(FMX_DENSE_F64, Q, b, b, W, b, b, n, gpart, H, nullptr, st));
 		E_TRY(fmx_dense_sym_eig(H, b, wv, V, st));
 		order_kernel<<<1, 1, 0, st>>>(wv, b, o.which == FMX_EIGEN_LM, perm, dsmall->theta);
