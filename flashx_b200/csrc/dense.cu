@@ -1257,114 +1257,211 @@ __global__ void __launch_bounds__(kJacobiThreads) jacobi_eig_kernel(const double
 	for (int i = t; i < b * b; i += blockDim.x) V[i] = Q[i / b][order[i % b]];
 }
 
-// The same decomposition for b <= 32 with fewer barriers and a shorter
-// serial chain per step.  A step applies each rotation to rows and columns
-// at once: with index i in pair (p, q) and new row i = k1(i) A[p] + k2(i) A[q]
-// (k = (c, -s) for i = p, (s, c) for i = q),
-//   A'[i][j] = sum_{x,y} k_x(i) k_y(j) A[r_x(i)][r_y(j)],
-//   Q'[i][j] = sum_y Q[i][r_y(j)] k_y(j),
-// and a rotated pair's own entries are set exactly: a_pp - t a_pq,
-// a_qq + t a_pq and 0.  Each of the 256 threads owns up to 4 fixed elements;
-// A and Q are double-buffered, so a step is two barriers: after the
-// rotation parameters, and after the new elements.  The parameters come
-// from d = a_qq - a_pp, e = 2 a_pq: t = sign(d) e / (|d| + sqrt(d^2 + e^2)),
-// c = 1 / sqrt(1 + t^2), s = t c (a square root, a division and a
-// reciprocal square root in the serial chain).
-constexpr int kJacobiSmallMax = 32;
-constexpr int kJacobiSmallThreads = 256;
+// ---------------------------------------------------------------------------
+// The same problem for b <= 32, with each thread owning a 2 x 2 block and one
+// barrier per Jacobi step.  In a step the m indices form m/2 pairs, and
+// thread (P, R) owns the entries of A with row in pair P and column in pair R
+// (and Q's entries of those rows and columns), so the step's two-sided
+// rotation J^T A J changes its block with only its two rotations:
+// about 3 shared-memory accesses per entry, against 14 when each thread owns
+// one entry and reads the rows and columns it mixes.  A 32-thread rotation
+// warp computes step s + 1's rotations meanwhile, from the same A and step
+// s's rotations: for each next pair it evaluates a_pp, a_qq and a_pq after
+// step s by the block formula itself (so they equal what the owners store).
+// Pairings (round robin) and the index tables are built once.  The angle:
+// t = sign(d) e / (|d| + sqrt(d^2 + e^2)), d = a_qq - a_pp, e = 2 a_pq,
+// evaluated in FP32 (hardware reciprocal square root and reciprocal) on d
+// and e scaled by a power of two.  An angle off by 1e-6 leaves a_pq at 1e-6
+// of its size instead of zero, which later steps remove.  c and s are then
+// normalised in FP64 by two Newton steps for c^2 + s^2 = 1 (multiply by
+// 3/2 - n/2, n = c^2 + s^2), so each rotation is orthogonal to FP64 rounding
+// and the eigenvalues keep FP64 accuracy.
+// ---------------------------------------------------------------------------
+constexpr int kJF = 32;
+constexpr int kJFHalf = kJF / 2;
+constexpr int kJFBlockThreads = kJFHalf * kJFHalf;   // 256 block owners at most
+constexpr int kJFThreads = kJFBlockThreads + 32;     // + the rotation warp
 
-__global__ void __launch_bounds__(kJacobiSmallThreads) jacobi_small_kernel(const double *__restrict__ H, int b,
+// c, s of the rotation that (nearly) zeroes a_pq (c = 1, s = 0 when a_pq = 0
+// or negligible against a_qq - a_pp).  New vectors: a' = c a - s q,
+// q' = s a + c q.
+__device__ __forceinline__ void jf_rotation(double app, double aqq, double apq, double &c, double &s)
+{
+	c = 1.0;
+	s = 0.0;
+	if (apq == 0.0) return;
+	const double d = aqq - app, e = 2.0 * apq;
+	const double M = fmax(fabs(d), fabs(e));
+	float df, ef;
+	if (M > 1e-30 && M < 1e30) {
+		df = float(d);                                 // t depends on e / d only
+		ef = float(e);
+	} else {
+		// 2^-k that brings M into [0.5, 1) (exponent field arithmetic, exact)
+		int ex = int((__double_as_longlong(M) >> 52) & 0x7ff) - 1022;
+		ex = max(-1021, min(1022, ex));
+		const double sc = __longlong_as_double((long long)(1023 - ex) << 52);
+		df = float(d * sc);
+		ef = float(e * sc);
+	}
+	if (ef == 0.f) return;
+	const float x = __fmaf_rn(df, df, ef * ef);        // > 0
+	const float r = x * rsqrtf(x);                     // sqrt(d^2 + e^2)
+	float t = __fdividef(ef, fabsf(df) + r);
+	if (df < 0.f) t = -t;
+	const float c32 = rsqrtf(__fmaf_rn(t, t, 1.f));
+	double cc = double(c32), ss = double(t) * double(c32);   // exact products of floats
+#pragma unroll
+	for (int it = 0; it < 2; it++) {
+		const double nrm = __fma_rn(cc, cc, ss * ss);
+		const double f = __fma_rn(-0.5, nrm, 1.5);
+		cc *= f;
+		ss *= f;
+	}
+	c = cc;
+	s = ss;
+}
+
+// The 2 x 2 block (rows aP, qP; columns aR, qR) of J^T A J: columns mixed by
+// pair R's rotation, then rows by pair P's.
+__device__ __forceinline__ void jf_block(double x00, double x01, double x10, double x11, double cP, double sP,
+		double cR, double sR, double &z00, double &z01, double &z10, double &z11)
+{
+	const double y00 = __fma_rn(-sR, x01, __dmul_rn(cR, x00));
+	const double y01 = __fma_rn(cR, x01, __dmul_rn(sR, x00));
+	const double y10 = __fma_rn(-sR, x11, __dmul_rn(cR, x10));
+	const double y11 = __fma_rn(cR, x11, __dmul_rn(sR, x10));
+	z00 = __fma_rn(-sP, y10, __dmul_rn(cP, y00));
+	z01 = __fma_rn(-sP, y11, __dmul_rn(cP, y01));
+	z10 = __fma_rn(cP, y10, __dmul_rn(sP, y00));
+	z11 = __fma_rn(cP, y11, __dmul_rn(sP, y01));
+}
+
+// Entry (role rp of pair P, role rr of pair R) of J^T A J (role 0: the
+// pair's lower index).
+__device__ __forceinline__ double jf_pick(const double (*A)[kJF + 1], int aP, int qP, int aR, int qR, double cP,
+		double sP, double cR, double sR, int rp, int rr)
+{
+	double z00, z01, z10, z11;
+	jf_block(A[aP][aR], A[aP][qR], A[qP][aR], A[qP][qR], cP, sP, cR, sR, z00, z01, z10, z11);
+	return rp ? (rr ? z11 : z10) : (rr ? z01 : z00);
+}
+
+__global__ void __launch_bounds__(kJFThreads) jacobi_fast_kernel(const double *__restrict__ H, int b,
 		double *__restrict__ w, double *__restrict__ V, int max_sweeps)
 {
-	constexpr int NT = kJacobiSmallThreads, NW = NT / 32;
-	constexpr int KP = kJacobiSmallMax * kJacobiSmallMax / NT;      // elements per thread at most (4)
-	__shared__ double Ab[2][kJacobiSmallMax][kJacobiSmallMax + 1], Qb[2][kJacobiSmallMax][kJacobiSmallMax + 1];
-	__shared__ double k1[kJacobiSmallMax], k2[kJacobiSmallMax], dg[kJacobiSmallMax];
-	__shared__ int r1[kJacobiSmallMax], r2[kJacobiSmallMax], mate[kJacobiSmallMax], order[kJacobiSmallMax];
+	constexpr int NW = kJFBlockThreads / 32;
+	__shared__ double Ab[2][kJF][kJF + 1], Qb[2][kJF][kJF + 1];
+	__shared__ double rc[2][kJFHalf], rs[2][kJFHalf];   // rotation of each pair slot: this step, the next
+	__shared__ uint8_t pa[kJF - 1][kJFHalf], pq[kJF - 1][kJFHalf];
+	__shared__ uint8_t sr[kJF - 1][kJF];                 // slot | role << 5 of each index, per step
+	__shared__ uint32_t nx[kJF - 1][kJFHalf];            // rotation warp: see below
+	__shared__ uint32_t nxi[kJF - 1][kJFHalf];
+	__shared__ int order[kJF];
 	__shared__ double red[2][NW];
 	const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
-	const int m = (b + 1) & ~1;                       // even size (pad with a zero row/column)
-	const int half = m / 2, mm = m * m;
-	int ei[KP], ej[KP];
-#pragma unroll
-	for (int u = 0; u < KP; u++) {
-		const int e = t + NT * u;
-		ei[u] = e < mm ? e / m : -1;
-		ej[u] = e < mm ? e % m : 0;
-	}
-	for (int e = t; e < mm; e += NT) {
+	const int m = (b + 1) & ~1;                         // even size (pad with a zero row/column)
+	const int half = m / 2, mm = m * m, steps = m - 1;
+	const bool owner = t < half * half;
+	const int P = owner ? t / half : 0, R = owner ? t % half : 0;
+	const bool rot = wid == NW && lane < half;          // the rotation warp's active lanes
+	for (int e = t; e < mm; e += kJFThreads) {
 		const int r = e / m, c = e % m;
 		Ab[0][r][c] = (r < b && c < b) ? 0.5 * (H[r * b + c] + H[c * b + r]) : 0.0;
 		Qb[0][r][c] = (r == c) ? 1.0 : 0.0;
 	}
-	if (t < kJacobiSmallMax) order[t] = t;            // complete even if the padding is not recognised
+	// round-robin tournament pairing of 0..m-1: step st, slot k
+	for (int e = t; e < steps * half; e += kJFThreads) {
+		const int st = e / half, k = e % half;
+		int a = k == 0 ? 0 : 1 + (k - 1 + st) % (m - 1);
+		int q = 1 + (m - 2 - k + st) % (m - 1);
+		if (a > q) { const int x = a; a = q; q = x; }
+		pa[st][k] = uint8_t(a);
+		pq[st][k] = uint8_t(q);
+		sr[st][a] = uint8_t(k);
+		sr[st][q] = uint8_t(k | 32);
+	}
+	if (t < kJF) order[t] = t;                          // complete even if the padding is not recognised
 	__syncthreads();
-	int cur = 0;
+	// rotation warp, slot k of step s: the pair (a, q) of step s + 1 (step 0
+	// after the last), packed a | q << 8 | (slot | role << 5 of a in step s)
+	// << 16 | (the same of q) << 24; and the two step-s pairs holding a and q,
+	// packed a1 | q1 << 8 | a2 << 16 | q2 << 24
+	for (int e = t; e < steps * half; e += kJFThreads) {
+		const int st = e / half, k = e % half;
+		const int ns = st + 1 < steps ? st + 1 : 0;
+		const int a = pa[ns][k], q = pq[ns][k];
+		const int ka = sr[st][a] & 31, kq = sr[st][q] & 31;
+		nx[st][k] = uint32_t(a) | (uint32_t(q) << 8) | (uint32_t(sr[st][a]) << 16) | (uint32_t(sr[st][q]) << 24);
+		nxi[st][k] = uint32_t(pa[st][ka]) | (uint32_t(pq[st][ka]) << 8) | (uint32_t(pa[st][kq]) << 16) |
+				(uint32_t(pq[st][kq]) << 24);
+	}
+	// step 0's rotations, from A itself
+	if (t < half) {
+		const int a = pa[0][t], q = pq[0][t];
+		double c, sn;
+		jf_rotation(Ab[0][a][a], Ab[0][q][q], Ab[0][a][q], c, sn);
+		rc[0][t] = c;
+		rs[0][t] = sn;
+	}
+	__syncthreads();
+	int cur = 0, par = 0;
 	for (int sweep = 0; sweep < max_sweeps; sweep++) {
 		double so = 0, sd = 0;
-#pragma unroll
-		for (int u = 0; u < KP; u++) {
-			if (ei[u] < 0) continue;
-			const double v = Ab[cur][ei[u]][ej[u]];
-			if (ei[u] == ej[u]) sd += v * v; else so += v * v;
+		if (owner) {
+			const int aP = pa[0][P], qP = pq[0][P], aR = pa[0][R], qR = pq[0][R];
+			const double x00 = Ab[cur][aP][aR], x01 = Ab[cur][aP][qR], x10 = Ab[cur][qP][aR], x11 = Ab[cur][qP][qR];
+			if (P == R) { sd = x00 * x00 + x11 * x11; so = x01 * x01 + x10 * x10; }
+			else so = x00 * x00 + x01 * x01 + x10 * x10 + x11 * x11;
 		}
 		for (int o = 16; o > 0; o >>= 1) {
 			so += __shfl_xor_sync(0xffffffffu, so, o);
 			sd += __shfl_xor_sync(0xffffffffu, sd, o);
 		}
-		if (lane == 0) { red[0][wid] = so; red[1][wid] = sd; }
+		if (wid < NW && lane == 0) { red[0][wid] = so; red[1][wid] = sd; }
 		__syncthreads();
 		so = 0; sd = 0;
 		for (int i = 0; i < NW; i++) { so += red[0][i]; sd += red[1][i]; }
-		// the same decision in every thread: off-diagonal norm below 1e-12 of
-		// the diagonal's (squared 1e-24), far below what the 1e-6 residuals
-		// of the solve need; a sweep more (to 1e-30) cost about 14 %
+		// the same decision in every thread (see kJacobiOff2)
 		if (so / (sd > 0 ? sd : 1.0) < kJacobiOff2) break;
-		for (int step = 0; step < m - 1; step++) {
-			const double (*A)[kJacobiSmallMax + 1] = Ab[cur];
-			const double (*Q)[kJacobiSmallMax + 1] = Qb[cur];
-			if (t < half) {
-				// round-robin tournament pairing of 0..m-1
-				int a = t == 0 ? 0 : 1 + (t - 1 + step) % (m - 1);
-				int q = 1 + (m - 2 - t + step) % (m - 1);
-				if (a > q) { const int x = a; a = q; q = x; }
-				const double app = A[a][a], aqq = A[q][q], apq = A[a][q];
-				double c = 1, sn = 0, tt = 0;
-				if (fabs(apq) > 1e-300) {
-					const double d = aqq - app, e = 2 * apq;
-					tt = (d >= 0 ? e : -e) / (fabs(d) + sqrt(d * d + e * e));
-					c = rsqrt(1 + tt * tt);
-					sn = tt * c;
-				}
-				r1[a] = a; r2[a] = q; k1[a] = c; k2[a] = -sn; dg[a] = -tt * apq; mate[a] = q;
-				r1[q] = a; r2[q] = q; k1[q] = sn; k2[q] = c; dg[q] = tt * apq; mate[q] = a;
-			}
-			__syncthreads();
-			double (*An)[kJacobiSmallMax + 1] = Ab[cur ^ 1];
-			double (*Qn)[kJacobiSmallMax + 1] = Qb[cur ^ 1];
-#pragma unroll
-			for (int u = 0; u < KP; u++) {
-				const int i = ei[u], j = ej[u];
-				if (i < 0) continue;
-				const int ja = r1[j], jb = r2[j];
-				const double ya = k1[j], yb = k2[j];
-				Qn[i][j] = Q[i][ja] * ya + Q[i][jb] * yb;
-				if (i == j) {
-					An[i][j] = A[i][i] + dg[i];
-				} else if (mate[i] == j) {
-					An[i][j] = 0.0;
-				} else {
-					const int ia = r1[i], ib = r2[i];
-					const double xa = k1[i], xb = k2[i];
-					An[i][j] = xa * (A[ia][ja] * ya + A[ia][jb] * yb) + xb * (A[ib][ja] * ya + A[ib][jb] * yb);
-				}
+		for (int step = 0; step < steps; step++) {
+			const double (*A)[kJF + 1] = Ab[cur];
+			const double *cs = rc[par], *ss = rs[par];
+			if (owner) {
+				const double (*Q)[kJF + 1] = Qb[cur];
+				double (*An)[kJF + 1] = Ab[cur ^ 1];
+				double (*Qn)[kJF + 1] = Qb[cur ^ 1];
+				const int aP = pa[step][P], qP = pq[step][P], aR = pa[step][R], qR = pq[step][R];
+				const double cP = cs[P], sP = ss[P], cR = cs[R], sR = ss[R];
+				double z00, z01, z10, z11;
+				jf_block(A[aP][aR], A[aP][qR], A[qP][aR], A[qP][qR], cP, sP, cR, sR, z00, z01, z10, z11);
+				An[aP][aR] = z00; An[aP][qR] = z01; An[qP][aR] = z10; An[qP][qR] = z11;
+				// Q J: rows aP and qP, columns of pair R
+				const double u0 = Q[aP][aR], v0 = Q[aP][qR], u1 = Q[qP][aR], v1 = Q[qP][qR];
+				Qn[aP][aR] = __fma_rn(-sR, v0, __dmul_rn(cR, u0));
+				Qn[aP][qR] = __fma_rn(cR, v0, __dmul_rn(sR, u0));
+				Qn[qP][aR] = __fma_rn(-sR, v1, __dmul_rn(cR, u1));
+				Qn[qP][qR] = __fma_rn(cR, v1, __dmul_rn(sR, u1));
+			} else if (rot) {
+				const uint32_t pk = nx[step][lane], pi = nxi[step][lane];
+				const int ka = (pk >> 16) & 31, ra = (pk >> 21) & 1, kq = (pk >> 24) & 31, rq = (pk >> 29) & 1;
+				const int a1 = pi & 0xff, q1 = (pi >> 8) & 0xff, a2 = (pi >> 16) & 0xff, q2 = pi >> 24;
+				const double c1 = cs[ka], s1 = ss[ka], c2 = cs[kq], s2 = ss[kq];
+				const double app = jf_pick(A, a1, q1, a1, q1, c1, s1, c1, s1, ra, ra);
+				const double aqq = jf_pick(A, a2, q2, a2, q2, c2, s2, c2, s2, rq, rq);
+				const double apq = jf_pick(A, a1, q1, a2, q2, c1, s1, c2, s2, ra, rq);
+				double c, sn;
+				jf_rotation(app, aqq, apq, c, sn);
+				rc[par ^ 1][lane] = c;
+				rs[par ^ 1][lane] = sn;
 			}
 			cur ^= 1;
+			par ^= 1;
 			__syncthreads();
 		}
 	}
-	const double (*A)[kJacobiSmallMax + 1] = Ab[cur];
-	const double (*Q)[kJacobiSmallMax + 1] = Qb[cur];
+	const double (*A)[kJF + 1] = Ab[cur];
+	const double (*Q)[kJF + 1] = Qb[cur];
 	// descending order of the b real eigenvalues (the padding one, if any, is dropped)
 	if (t < 32) {
 		const bool real = lane < m && !((m != b) && (fabs(Q[b][lane]) > 0.5));
@@ -1381,8 +1478,8 @@ __global__ void __launch_bounds__(kJacobiSmallThreads) jacobi_small_kernel(const
 		}
 	}
 	__syncthreads();
-	for (int i = t; i < b; i += NT) w[i] = A[order[i]][order[i]];
-	for (int i = t; i < b * b; i += NT) V[i] = Q[i / b][order[i % b]];
+	for (int i = t; i < b; i += kJFThreads) w[i] = A[order[i]][order[i]];
+	for (int i = t; i < b * b; i += kJFThreads) V[i] = Q[i / b][order[i % b]];
 }
 
 // ---------------------------------------------------------------------------
@@ -1882,11 +1979,8 @@ int fmx_dense_sym_eig(const double *H, int b, double *w, double *V, void *stream
 {
 	if (!H || !w || !V) return set_error(FMX_ERR_INVAL, "null argument");
 	if (b < 1 || b > 64) return set_error(FMX_ERR_UNSUPPORTED, "b in 1..64");
-	// the double-buffered kernel for b <= 16 (86 against 105 us on a random
-	// 16 x 16 problem); at b = 24 the two-phase kernel is faster (196 against
-	// 222 us): 2.25 elements per thread lengthen each step of the former
-	if (b <= 16) {
-		jacobi_small_kernel<<<1, kJacobiSmallThreads, 0, static_cast<cudaStream_t>(stream)>>>(H, b, w, V, 30);
+	if (b <= kJF) {
+		jacobi_fast_kernel<<<1, kJFThreads, 0, static_cast<cudaStream_t>(stream)>>>(H, b, w, V, 30);
 		DCUDA_TRY(cudaGetLastError());
 		return FMX_OK;
 	}
