@@ -796,6 +796,79 @@ __global__ void pack_hot_kernel(const int32_t *hot_col, uint32_t n_hot, const XT
 	}
 }
 
+// The same in 16-byte units (rows of whole units, 16-byte aligned), with 4
+// units in flight per thread: the copy is a gather of random rows of X, and
+// one 4-byte element per thread left it at a third of the bandwidth its
+// bytes allow.
+template <class XT, class A, bool SCALE_IN>
+__global__ void pack_hot_vec_kernel(const int32_t *hot_col, uint32_t n_hot, const XT *X, int64_t ldx, int units,
+		XT *xhot, int hot_ld, const A *s_in)
+{
+	constexpr int E = int(16 / sizeof(XT));
+	constexpr int D = 4;
+	const uint64_t total = uint64_t(n_hot + 1) * units;
+	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+	for (uint64_t t0 = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; t0 < total; t0 += D * stride) {
+		uint4 v[D];
+		int32_t c[D];
+#pragma unroll
+		for (int q = 0; q < D; q++) {
+			const uint64_t t = t0 + q * stride;
+			v[q] = make_uint4(0, 0, 0, 0);
+			c[q] = -1;
+			if (t < total) {
+				const uint32_t sl = uint32_t(t / units);
+				const int u = int(t - uint64_t(sl) * units);
+				if (sl > 0) {
+					c[q] = __ldg(hot_col + sl - 1);
+					v[q] = __ldg(reinterpret_cast<const uint4 *>(X + int64_t(c[q]) * ldx) + u);
+				}
+			}
+		}
+#pragma unroll
+		for (int q = 0; q < D; q++) {
+			const uint64_t t = t0 + q * stride;
+			if (t >= total) continue;
+			const uint32_t sl = uint32_t(t / units);
+			const int u = int(t - uint64_t(sl) * units);
+			if constexpr (SCALE_IN) {
+				if (c[q] >= 0) {
+					XT e[E];
+					memcpy(e, &v[q], 16);
+					const A sc = s_in[c[q]];
+#pragma unroll
+					for (int i = 0; i < E; i++) e[i] = from_acc<XT, A>(acc_mul(to_acc<A>(e[i]), sc));
+					memcpy(&v[q], e, 16);
+				}
+			}
+			*reinterpret_cast<uint4 *>(xhot + int64_t(sl) * hot_ld + int64_t(u) * E) = v[q];
+		}
+	}
+}
+
+// The hot pack of one panel: 16-byte units when the rows allow it.
+template <class XT, class A>
+static int launch_pack(const gpu_part &p, const XT *X, int64_t ldx, int kp, XT *xhot, int hot_ld, const A *s_in,
+		cudaStream_t st)
+{
+	const bool vec = (kp * sizeof(XT)) % 16 == 0 && (ldx * sizeof(XT)) % 16 == 0 && (hot_ld * sizeof(XT)) % 16 == 0 &&
+			(reinterpret_cast<uintptr_t>(X) & 15) == 0 && (reinterpret_cast<uintptr_t>(xhot) & 15) == 0;
+	if (vec) {
+		const int units = int(kp * sizeof(XT) / 16);
+		const uint64_t total = uint64_t(p.n_hot + 1) * units;
+		const unsigned pb = unsigned(std::max<uint64_t>(1, std::min<uint64_t>((total + 1023) / 1024, 148ull * 8)));
+		if (s_in) pack_hot_vec_kernel<XT, A, true><<<pb, 256, 0, st>>>(p.hot_col, p.n_hot, X, ldx, units, xhot, hot_ld, s_in);
+		else pack_hot_vec_kernel<XT, A, false><<<pb, 256, 0, st>>>(p.hot_col, p.n_hot, X, ldx, units, xhot, hot_ld, nullptr);
+	} else {
+		const uint64_t total = uint64_t(p.n_hot + 1) * kp;
+		const unsigned pb = unsigned(std::min<uint64_t>((total + 255) / 256, 148ull * 16));
+		if (s_in) pack_hot_kernel<XT, A, true><<<pb, 256, 0, st>>>(p.hot_col, p.n_hot, X, ldx, kp, xhot, hot_ld, s_in);
+		else pack_hot_kernel<XT, A, false><<<pb, 256, 0, st>>>(p.hot_col, p.n_hot, X, ldx, kp, xhot, hot_ld, nullptr);
+	}
+	CUDA_TRY(cudaGetLastError());
+	return FMX_OK;
+}
+
 // Part `part` of P adds chunks part, part + P, ... of one column unit (a
 // float4 when vec, else one element) into two running sums (even and odd
 // steps).
@@ -1347,15 +1420,9 @@ static int launch_wide(const gpu_part &p, const spmm_args &a, cudaStream_t st)
 template <class XT, class YT, class A, class WT, int VEC, int NV>
 static int launch_t(const gpu_part &p, spmm_args a, bool sin, bool sout, cudaStream_t st, bool wide = false)
 {
-	{
-		const uint64_t total = uint64_t(p.n_hot + 1) * a.k;
-		const unsigned pb = unsigned(std::min<uint64_t>((total + 255) / 256, 148ull * 16));
-		if (sin) pack_hot_kernel<XT, A, true><<<pb, 256, 0, st>>>(p.hot_col, p.n_hot, static_cast<const XT *>(a.X),
-				a.ldx, a.k, static_cast<XT *>(p.xhot), a.hot_ld, static_cast<const A *>(a.s_in));
-		else pack_hot_kernel<XT, A, false><<<pb, 256, 0, st>>>(p.hot_col, p.n_hot, static_cast<const XT *>(a.X),
-				a.ldx, a.k, static_cast<XT *>(p.xhot), a.hot_ld, nullptr);
-		CUDA_TRY(cudaGetLastError());
-	}
+	if (int rc = launch_pack<XT, A>(p, static_cast<const XT *>(a.X), a.ldx, a.k, static_cast<XT *>(p.xhot), a.hot_ld,
+			sin ? static_cast<const A *>(a.s_in) : nullptr, st))
+		return rc;
 	int rc = over_slices(p, a, st, [&](const spmm_args &sa) -> int {
 		if constexpr (std::is_same<A, float>::value &&
 				(sizeof(XT) == 4 || (sizeof(YT) == 2 && std::is_void<WT>::value)) &&
@@ -2076,12 +2143,8 @@ static int run_noalloc(const gpu_part &p, const float *X, int64_t ldx, float *Y,
 		a.partial = partial;
 		a.ldx = ldx; a.ldy = ldy; a.k = kp;
 		a.n_ranges = p.n_ranges;
-		const uint64_t total = uint64_t(p.n_hot + 1) * kp;
-		const unsigned pb = unsigned(std::min<uint64_t>((total + 255) / 256, 148ull * 16));
-		pack_hot_kernel<float, float, false><<<pb, 256, 0, st>>>(p.hot_col, p.n_hot, X + c0, ldx, kp,
-				static_cast<float *>(xhot), kp, nullptr);
-		CUDA_TRY(cudaGetLastError());
-		int rc;
+		int rc = launch_pack<float, float>(p, X + c0, ldx, kp, static_cast<float *>(xhot), kp, nullptr, st);
+		if (rc) return rc;
 		if (vec_ok) {
 			a.G = kp / VEC;
 			a.R = 32 / a.G;
