@@ -997,7 +997,7 @@ def main():
                                     "scratch_bytes": scratch_bytes}},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
-                         "kernel": "pack_hot_kernel + spmm_wide_kernel + spmm_fixup kernels, per fmx_spmm call",
+                         "kernel": "pack_hot_vec_kernel + spmm_wide_kernel + spmm_fixup kernels, per fmx_spmm call",
                          "traffic": traffic},
             "cpu_baseline": cpu,
             "e2e": e2e,
