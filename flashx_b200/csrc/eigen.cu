@@ -119,7 +119,9 @@ __global__ void cheb_kernel(const float *__restrict__ W, const YT *__restrict__ 
 
 // One step of the filter in correction form, on flat n x b blocks:
 //   O = alpha W - ac0 E - beta P + cr[col] R + cx[col] X
-// (each of W, E, P, R, X may be absent)
+// (each of W, E, P, R, X may be absent); R FP32 or BF16.  With Rb, the step
+// also writes R rounded to BF16 there (the first step of a pass, so that the
+// later BF16 steps read half the bytes of R).
 struct col_coefs {
 	float r[kMaxB];
 	float x[kMaxB];
@@ -173,10 +175,10 @@ __device__ __forceinline__ void st8(__nv_bfloat16 *p, const float (&v)[8])
 	*reinterpret_cast<uint4 *>(p) = make_uint4(w[0], w[1], w[2], w[3]);
 }
 
-template <class WT, class ET, class PT, class OT>
+template <class WT, class ET, class PT, class RT, class OT>
 __global__ void corr_kernel(const WT *__restrict__ W, const ET *__restrict__ E, const PT *__restrict__ P,
-		const float *__restrict__ R, const float *__restrict__ X, OT *__restrict__ O, int64_t count, int b,
-		float alpha, float ac0, float beta, col_coefs cf)
+		const RT *__restrict__ R, const float *__restrict__ X, OT *__restrict__ O, int64_t count, int b,
+		float alpha, float ac0, float beta, col_coefs cf, __nv_bfloat16 *__restrict__ Rb)
 {
 	const bool pow2 = (b & (b - 1)) == 0;
 	const int64_t tstride = int64_t(gridDim.x) * blockDim.x;
@@ -206,6 +208,7 @@ __global__ void corr_kernel(const WT *__restrict__ W, const ET *__restrict__ E, 
 			}
 			if (R) {
 				ld8(R + i, t);
+				if (Rb) st8(Rb + i, t);
 #pragma unroll
 				for (int q = 0; q < 8; q++) v[q] += cf.r[col + q] * t[q];
 			}
@@ -238,6 +241,7 @@ __global__ void corr_kernel(const WT *__restrict__ W, const ET *__restrict__ E, 
 			}
 			if (R) {
 				const float4 t = ld4(R + i);
+				if (Rb) st4(Rb + i, t);
 				v.x += cf.r[col] * t.x; v.y += cf.r[col + 1] * t.y; v.z += cf.r[col + 2] * t.z; v.w += cf.r[col + 3] * t.w;
 			}
 			if (X) {
@@ -254,7 +258,11 @@ __global__ void corr_kernel(const WT *__restrict__ W, const ET *__restrict__ E, 
 		if (W) v = alpha * ldf(W + i);
 		if (E) v -= ac0 * ldf(E + i);
 		if (P) v -= beta * ldf(P + i);
-		if (R) v += cf.r[col] * R[i];
+		if (R) {
+			const float r = ldf(R + i);
+			if (Rb) stf(Rb + i, r);
+			v += cf.r[col] * r;
+		}
 		if (X) v += cf.x[col] * X[i];
 		stf(O + i, v);
 	}
@@ -680,6 +688,7 @@ struct solver {
 	cudaStream_t st;
 	workspace ws;
 	float *X = nullptr, *NX = nullptr, *W = nullptr, *B[3] = {nullptr, nullptr, nullptr};
+	__nv_bfloat16 *Rb = nullptr;     // mixed precision: R in BF16 for the correction steps
 	double *G = nullptr, *T = nullptr, *H = nullptr, *wv = nullptr, *V = nullptr, *eye = nullptr;
 	double *part = nullptr, *dsmall_theta = nullptr;
 	float *Tf = nullptr, *gpart = nullptr;
@@ -720,6 +729,7 @@ struct solver {
 		E_TRY(ws.get(&NX, nb));
 		E_TRY(ws.get(&W, nb));
 		for (auto &p : B) E_TRY(ws.get(&p, nb));
+		if (o.precision == FMX_EIGEN_MIXED) E_TRY(ws.get(&Rb, nb));
 		E_TRY(ws.get(&G, b * b));
 		E_TRY(ws.get(&T, b * b));
 		E_TRY(ws.get(&H, b * b));
@@ -889,13 +899,13 @@ struct solver {
 		return FMX_OK;
 	}
 
-	template <class WT, class ET, class PT, class OT>
-	int corr_step(const WT *Wm, const ET *E, const PT *P, const float *R, const float *Xs, OT *Out, float alpha,
-			float ac0, float beta, const col_coefs &cf)
+	template <class WT, class ET, class PT, class RT, class OT>
+	int corr_step(const WT *Wm, const ET *E, const PT *P, const RT *R, const float *Xs, OT *Out, float alpha,
+			float ac0, float beta, const col_coefs &cf, __nv_bfloat16 *Rb = nullptr)
 	{
 		const int64_t cnt = n * b;
-		corr_kernel<WT, ET, PT, OT><<<flat_grid(cnt), kThreads, 0, st>>>(Wm, E, P, R, Xs, Out, cnt, b, alpha, ac0, beta,
-				cf);
+		corr_kernel<WT, ET, PT, RT, OT><<<flat_grid(cnt), kThreads, 0, st>>>(Wm, E, P, R, Xs, Out, cnt, b, alpha, ac0,
+				beta, cf, Rb);
 		ECUDA_TRY(cudaGetLastError());
 		return FMX_OK;
 	}
@@ -930,8 +940,10 @@ struct solver {
 			*out_k = 0;
 			return FMX_OK;
 		}
+		// E_1, and R in BF16 for the middle steps (their BF16 operands carry
+		// the same relative rounding)
 		E_TRY(corr_step((const float *)nullptr, (const float *)nullptr, (const float *)nullptr, R,
-				(const float *)nullptr, (bf *)B[0], 0.f, 0.f, 0.f, cf));
+				(const float *)nullptr, (bf *)B[0], 0.f, 0.f, 0.f, cf, Rb));
 		int cur = 0, prev = -1;
 		double sj = s1;
 		for (int jdeg = 2; jdeg <= mdeg; jdeg++) {
@@ -951,7 +963,7 @@ struct solver {
 			const float a = float(alpha), ac = float(alpha * c0), bt = float(beta);
 			const bf *Wb = (const bf *)W;
 			if (last) E_TRY(corr_step(Wb, E, P, R, X, B[nxt], a, ac, bt, cf));
-			else E_TRY(corr_step(Wb, E, P, R, (const float *)nullptr, (bf *)B[nxt], a, ac, bt, cf));
+			else E_TRY(corr_step(Wb, E, P, (const bf *)Rb, (const float *)nullptr, (bf *)B[nxt], a, ac, bt, cf));
 			prev = cur;
 			cur = nxt;
 			sj = sn;
