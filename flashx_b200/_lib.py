@@ -92,6 +92,7 @@ _SIGS = {
     "fmx_matrix_free": (_int, [_vp]),
     "fmx_spmm": (_int, [_vp, _int, _vp, _i64, _int, _vp, _i64, _i64, _vp, _vp, _vp]),
     "fmx_spmm_host": (_int, [_vp, _int, _vp, _i64, _int, _vp, _i64, _i64]),
+    "fmx_spmm_host_async": (_int, [_vp, _int, _vp, _i64, _int, _vp, _i64, _i64, _vp]),
     "fmx_spmm_noalloc": (_int, [_vp, _vp, _i64, _vp, _i64, _i64, _vp]),
     "fmx_matrix_schedule": (_int, [_vp, _P(_u64), _P(_u64), _P(_u64), _P(_u64)]),
     "fmx_matrix_hot": (_int, [_vp, _P(_u64), _P(_u64), _P(_u64)]),

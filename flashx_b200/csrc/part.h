@@ -119,6 +119,12 @@ struct gpu_part {
 	std::mutex stage_mu;
 	void *stage_x = nullptr, *stage_y = nullptr;
 	size_t stage_xb = 0, stage_yb = 0;
+	// fmx_spmm_host_async: staging per stream (grow-only; `done` is recorded
+	// after each call's copy of Y), and the event that orders the calls'
+	// SpMMs, which share the scratch above (guarded by stage_mu)
+	struct async_stage { cudaStream_t st; void *x, *y; size_t xb, yb; cudaEvent_t done; };
+	std::vector<async_stage> async_stages;
+	cudaEvent_t ev_scratch = nullptr;
 	~gpu_part() {
 		int cur = 0;
 		cudaGetDevice(&cur);
@@ -129,8 +135,13 @@ struct gpu_part {
 			if (p) cudaFree(p);
 		if (h_col) cudaFreeHost(h_col);
 		if (h_val) cudaFreeHost(h_val);
-		for (cudaEvent_t e : {ev_start, ev_copied[0], ev_copied[1], ev_free[0], ev_free[1]})
+		for (cudaEvent_t e : {ev_start, ev_copied[0], ev_copied[1], ev_free[0], ev_free[1], ev_scratch})
 			if (e) cudaEventDestroy(e);
+		for (async_stage &a : async_stages) {
+			if (a.x) cudaFree(a.x);
+			if (a.y) cudaFree(a.y);
+			if (a.done) cudaEventDestroy(a.done);
+		}
 		if (copy_st) cudaStreamDestroy(copy_st);
 		cudaSetDevice(cur);
 	}

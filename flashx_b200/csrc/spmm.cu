@@ -1989,6 +1989,67 @@ int fmx_spmm_host(const fmx_matrix *m, int x_type, const void *X_host, int64_t l
 	return rc;
 }
 
+int fmx_spmm_host_async(const fmx_matrix *m, int x_type, const void *X_host, int64_t ldx, int y_type,
+		void *Y_host, int64_t ldy, int64_t k, void *stream)
+{
+	if (!m || !m->a || !X_host || !Y_host) return set_error(FMX_ERR_INVAL, "null argument");
+	size_t xs = dtype_size(x_type), ys = dtype_size(y_type);
+	if (!xs || !ys) return set_error(FMX_ERR_TYPE, "unknown dtype");
+	if (k <= 0 || ldx < k || ldy < k) return set_error(FMX_ERR_DIM, "bad k / leading dimensions");
+	gpu_part &p = *m->a;
+	cudaStream_t st = static_cast<cudaStream_t>(stream);
+	std::lock_guard<std::mutex> guard(p.stage_mu);
+	int cur = 0;
+	cudaGetDevice(&cur);
+	CUDA_TRY(cudaSetDevice(p.device));
+	const size_t xb = size_t(p.ncols) * k * xs, yb = size_t(p.nrows) * k * ys;
+	int rc = FMX_OK;
+	gpu_part::async_stage *sg = nullptr;
+	for (gpu_part::async_stage &a : p.async_stages)
+		if (a.st == st) sg = &a;
+	if (!sg) {
+		p.async_stages.push_back(gpu_part::async_stage{st, nullptr, nullptr, 0, 0, nullptr});
+		sg = &p.async_stages.back();
+		if (cudaEventCreateWithFlags(&sg->done, cudaEventDisableTiming) != cudaSuccess)
+			rc = set_error(FMX_ERR_CUDA, "event creation failed");
+	}
+	if (!rc && !p.ev_scratch && cudaEventCreateWithFlags(&p.ev_scratch, cudaEventDisableTiming) != cudaSuccess)
+		rc = set_error(FMX_ERR_CUDA, "event creation failed");
+	// the stream's earlier calls must be through their copies before the
+	// staging buffers are reused (a stream handle can be recycled)
+	if (!rc && cudaStreamWaitEvent(st, sg->done, 0) != cudaSuccess) rc = set_error(FMX_ERR_CUDA, "stream wait failed");
+	auto grow = [&](void *&buf, size_t &have, size_t need) -> int {
+		if (have >= need) return FMX_OK;
+		if (buf) {
+			cudaStreamSynchronize(st);
+			cudaFree(buf);
+		}
+		buf = nullptr; have = 0;
+		if (cudaMalloc(&buf, need) != cudaSuccess) return set_error(FMX_ERR_OOM, "cudaMalloc of %zu staging bytes failed", need);
+		have = need;
+		return FMX_OK;
+	};
+	if (!rc) rc = grow(sg->x, sg->xb, xb);
+	if (!rc) rc = grow(sg->y, sg->yb, yb);
+	auto copy = [&](void *dst, size_t dpitch, const void *src, size_t spitch, size_t width, size_t rows,
+			cudaMemcpyKind kind) {
+		if (dpitch == width && spitch == width) return cudaMemcpyAsync(dst, src, width * rows, kind, st);
+		return cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, rows, kind, st);
+	};
+	if (!rc && copy(sg->x, k * xs, X_host, ldx * xs, k * xs, p.ncols, cudaMemcpyHostToDevice) != cudaSuccess)
+		rc = set_error(FMX_ERR_CUDA, "copy of X to the device failed");
+	// the SpMMs of calls on different streams share the matrix's scratch:
+	// each waits for the one issued before it
+	if (!rc && cudaStreamWaitEvent(st, p.ev_scratch, 0) != cudaSuccess) rc = set_error(FMX_ERR_CUDA, "stream wait failed");
+	if (!rc) rc = spmm_part(p, x_type, sg->x, k, y_type, sg->y, k, k, nullptr, nullptr, st);
+	if (!rc && cudaEventRecord(p.ev_scratch, st) != cudaSuccess) rc = set_error(FMX_ERR_CUDA, "event record failed");
+	if (!rc && copy(Y_host, ldy * ys, sg->y, k * ys, k * ys, p.nrows, cudaMemcpyDeviceToHost) != cudaSuccess)
+		rc = set_error(FMX_ERR_CUDA, "copy of Y to the host failed");
+	if (!rc && cudaEventRecord(sg->done, st) != cudaSuccess) rc = set_error(FMX_ERR_CUDA, "event record failed");
+	cudaSetDevice(cur);
+	return rc;
+}
+
 int fmx_matrix_hot(const fmx_matrix *m, uint64_t *n_hot_cols, uint64_t *hot_entries, uint64_t *scratch_bytes)
 {
 	if (!m || !m->a) return set_error(FMX_ERR_INVAL, "null matrix");

@@ -358,6 +358,22 @@ class sparse_matrix:
         return Y
 
 
+    def multiply_host_async(self, X, Y, stream):
+        """SpMM on host (numpy) buffers, asynchronous on `stream` (a CUDA
+        stream handle): X is copied in and Y out when the stream gets there.
+        Keep X and Y alive (and pinned, for asynchronous copies) until the
+        stream is synchronised."""
+        X2 = X.reshape(X.shape[0], -1)
+        Y2 = Y.reshape(Y.shape[0], -1)
+        if not (X2.flags.c_contiguous and Y2.flags.c_contiguous):
+            raise ValueError("multiply_host_async takes C-contiguous arrays")
+        code = {np.dtype(np.float32): _lib.F32, np.dtype(np.float64): _lib.F64,
+                np.dtype(np.int32): _lib.I32, np.dtype(np.int64): _lib.I64}[X.dtype]
+        check(lib.fmx_spmm_host_async(self._h, code, X2.ctypes.data, X2.shape[1], code, Y2.ctypes.data,
+                                      Y2.shape[1], X2.shape[1], stream))
+        return Y
+
+
 def create_2d_matrix(src, dst, vals=None, block_size=(16384, 16384), is_sym=True, device=0,
                      nrows=0, ncols=0, ref_value_layout=False, return_images=False):
     """fm::create_2d_matrix (matrix/fm_utils.cpp:726-841): edge list -> matrix.

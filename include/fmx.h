@@ -231,6 +231,23 @@ int fmx_spmm_noalloc(const fmx_matrix *m, const float *X, int64_t ldx, float *Y,
 int fmx_spmm_host(const fmx_matrix *m, int x_type, const void *X_host, int64_t ldx,
                   int y_type, void *Y_host, int64_t ldy, int64_t k);
 
+/* Host-buffer SpMM, asynchronous (no counterpart in the reference, whose
+ * multiply is synchronous): enqueues on `stream` the copy of X to the device,
+ * the SpMM and the copy of Y back, and returns.  X_host and Y_host must stay
+ * valid until the stream has reached the end of the call (synchronise the
+ * stream or wait on an event recorded after it).  With pinned host memory
+ * (cudaHostAlloc, cudaHostRegister) the copies are asynchronous; pageable
+ * memory makes them synchronous.  Each stream gets its own device staging
+ * for X and Y, kept by the matrix (grow-only) until it is freed, so calls
+ * issued alternately on two streams overlap one call's copy of Y with the
+ * next call's copy of X (PCIe carries both directions at once).  The SpMMs
+ * of these calls run one after another, ordered by an event, because they
+ * share the matrix's scratch; they are not ordered against fmx_spmm calls
+ * on other streams.  Calls on one matrix from several host threads are
+ * serialised by a lock, but their stream order is the caller's to set. */
+int fmx_spmm_host_async(const fmx_matrix *m, int x_type, const void *X_host, int64_t ldx,
+                        int y_type, void *Y_host, int64_t ldy, int64_t k, void *stream);
+
 /* Work decomposition of the resident matrix: rows summed by one lane group,
  * work ranges (runs of whole rows, or chunks of rows longer than
  * FMX_EXACT_ROW_MAX), rows finished by the chunk-sum pass, and kernel

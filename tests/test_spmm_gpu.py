@@ -257,6 +257,37 @@ def test_host_buffers_e2e(torch_cuda):
     assert np.array_equal(m.multiply_host(X), oracle.spmm(idx, mat, X))
 
 
+def test_host_buffers_async_two_streams(torch_cuda):
+    """fmx_spmm_host_async: six calls in flight on two streams, each with its
+    own pinned X and Y; every Y equals the oracle's (integer-valued X, so
+    exact), and a recycled stream reuses its staging."""
+    torch = torch_cuda
+    src, dst = _graph(20000, 100000, 23, ((7, 15000), (11, 900)))
+    idx, mat = oracle.build_image(src, dst, None, block=(4096, 4096), dedup=True)
+    m = sparse_matrix.create(matrix_image.from_bytes(idx, mat), None)
+    rng = np.random.default_rng(5)
+    streams = [torch.cuda.Stream(), torch.cuda.Stream()]
+    xs, ys, want = [], [], []
+    for i in range(6):
+        x = torch.from_numpy(rng.integers(-8, 9, (20000, 16)).astype(np.float32)).pin_memory()
+        y = torch.full((20000, 16), float("nan")).pin_memory()
+        xs.append(x)
+        ys.append(y)
+        want.append(oracle.spmm(idx, mat, x.numpy()))
+    for i in range(6):
+        m.multiply_host_async(xs[i].numpy(), ys[i].numpy(), streams[i % 2].cuda_stream)
+    for s in streams:
+        s.synchronize()
+    for i in range(6):
+        assert np.array_equal(ys[i].numpy(), want[i]), i
+    del streams
+    s3 = torch.cuda.Stream()
+    y3 = torch.full((20000, 16), float("nan")).pin_memory()
+    m.multiply_host_async(xs[0].numpy(), y3.numpy(), s3.cuda_stream)
+    s3.synchronize()
+    assert np.array_equal(y3.numpy(), want[0])
+
+
 def test_multiply_errors(torch_cuda):
     """Dimension and type mismatches return False, like the reference."""
     torch = torch_cuda
