@@ -63,6 +63,7 @@ def parse():
     p.add_argument("--skip-streamed", action="store_true")
     p.add_argument("--eig-scale", type=int, default=22, help="R-MAT scale of the eigensolver workload")
     p.add_argument("--eig-sbm", type=int, default=20, help="held-out SBM graphs for the learned warm start")
+    p.add_argument("--eig-reps", type=int, default=5, help="timed solves per mode (after one warm-up)")
     p.add_argument("--large", action="store_true",
                    help="run only the large single-GPU configuration (R-MAT scale 26: SpMM k=16 and 32, top-16 "
                         "eigensolve plain / mixed / learned start) and print its JSON line")
@@ -71,6 +72,9 @@ def parse():
     p.add_argument("--dense-only", action="store_true",
                    help="run only the eigensolver's dense tensor-core kernels (n = 2^22, 16 columns) and print "
                         "their JSON object")
+    p.add_argument("--eigen-only", action="store_true",
+                   help="run only the eigensolver configuration (and --eig-sbm held-out SBM graphs) and print "
+                        "its JSON object")
     p.add_argument("--skip-large", action="store_true")
     p.add_argument("--large-scale", type=int, default=26)
     return p.parse_args()
@@ -460,10 +464,12 @@ def eigen_measure(a, dev):
     results = {}
     out = {"workload": f"rmat-s{a.eig_scale}-ef16-symmetrised-na-top8-block16-tol1e-6", "n": n,
            "nnz": int(m.get_nnz()), "build_s": round(time.time() - t0, 2),
-           "timing": "median of 5 after 1 warm-up, CUDA events around the whole solve (host loop included)"}
+           "timing": f"median of {a.eig_reps} after 1 warm-up, CUDA events around the whole solve (host loop included)"}
     for prec in ("plain", "mixed"):
         o = ws.eigen_opts(8, 1e-6, prec)
-        ms, r = _timed_solve(torch, dev, lambda: compute_eigen(op, True, o))
+        torch.cuda.nvtx.range_push(f"eigen_{prec}")     # for profiler filters (ncu --nvtx-include)
+        ms, r = _timed_solve(torch, dev, lambda: compute_eigen(op, True, o), reps=a.eig_reps)
+        torch.cuda.nvtx.range_pop()
         out[prec] = _solve_summary(ms, r)
         results[prec] = r
     out["speedup_mixed_vs_plain"] = round(out["plain"]["ms"] / out["mixed"]["ms"], 3)
@@ -473,7 +479,9 @@ def eigen_measure(a, dev):
         return out
     net = ws.warm_start_net.load(weights, dev.index)
     o = ws.eigen_opts(8, 1e-6, "mixed")
-    ms, r = _timed_solve(torch, dev, lambda: compute_eigen(op, True, o, X0=net.start_block(op)))
+    torch.cuda.nvtx.range_push("eigen_mixed_learned")
+    ms, r = _timed_solve(torch, dev, lambda: compute_eigen(op, True, o, X0=net.start_block(op)), reps=a.eig_reps)
+    torch.cuda.nvtx.range_pop()
     out["mixed_learned"] = _solve_summary(ms, r)
     out["mixed_learned"]["spmm_calls"] += ws.SPMM_PER_START
     out["speedup_learned_mixed_vs_plain"] = round(out["plain"]["ms"] / ms, 3)
@@ -488,6 +496,8 @@ def eigen_measure(a, dev):
         e["residual"] = [float(f"{v:.3e}") for v in res.residuals]
         out[name]["errors"] = e
     del rows, cols, results, op, m
+    if a.eig_sbm <= 0:
+        return out
     rows = []
     for i in range(a.eig_sbm):
         inst = ws.sbm_instance(30_000_000 + i, solve=False)
@@ -839,6 +849,11 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if a.impl == "reference":
         return run_reference(a, rank, world)
+    if a.eigen_only:
+        if rank == 0:
+            import torch
+            print(json.dumps(eigen_measure(a, torch.device("cuda", local))), flush=True)
+        return
     if a.dense_only:
         if rank == 0:
             import torch
