@@ -119,11 +119,16 @@ struct gpu_part {
 	std::mutex stage_mu;
 	void *stage_x = nullptr, *stage_y = nullptr;
 	size_t stage_xb = 0, stage_yb = 0;
-	// fmx_spmm_host_async: staging per stream (grow-only; `done` is recorded
-	// after each call's copy of Y), and the event that orders the calls'
-	// SpMMs, which share the scratch above (guarded by stage_mu)
-	struct async_stage { cudaStream_t st; void *x, *y; size_t xb, yb; cudaEvent_t done; };
-	std::vector<async_stage> async_stages;
+	// fmx_spmm_host_async (guarded by stage_mu): a ring of two staging slots
+	// (grow-only), one stream for the copies of X in and one for the copies
+	// of Y out, so each direction runs back to back; per slot, events for X
+	// arrived, the SpMM done (X consumed, Y ready) and Y copied out; and the
+	// event that orders the calls' SpMMs, which share the scratch above
+	struct async_slot { void *x = nullptr, *y = nullptr; size_t xb = 0, yb = 0;
+		cudaEvent_t x_ready = nullptr, spmm_done = nullptr, y_out = nullptr; };
+	async_slot aslot[2];
+	unsigned anext = 0;
+	cudaStream_t h2d_st = nullptr, d2h_st = nullptr;
 	cudaEvent_t ev_scratch = nullptr;
 	~gpu_part() {
 		int cur = 0;
@@ -137,11 +142,14 @@ struct gpu_part {
 		if (h_val) cudaFreeHost(h_val);
 		for (cudaEvent_t e : {ev_start, ev_copied[0], ev_copied[1], ev_free[0], ev_free[1], ev_scratch})
 			if (e) cudaEventDestroy(e);
-		for (async_stage &a : async_stages) {
+		for (async_slot &a : aslot) {
 			if (a.x) cudaFree(a.x);
 			if (a.y) cudaFree(a.y);
-			if (a.done) cudaEventDestroy(a.done);
+			for (cudaEvent_t e : {a.x_ready, a.spmm_done, a.y_out})
+				if (e) cudaEventDestroy(e);
 		}
+		for (cudaStream_t s : {h2d_st, d2h_st})
+			if (s) cudaStreamDestroy(s);
 		if (copy_st) cudaStreamDestroy(copy_st);
 		cudaSetDevice(cur);
 	}

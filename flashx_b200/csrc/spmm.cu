@@ -2004,48 +2004,69 @@ int fmx_spmm_host_async(const fmx_matrix *m, int x_type, const void *X_host, int
 	CUDA_TRY(cudaSetDevice(p.device));
 	const size_t xb = size_t(p.ncols) * k * xs, yb = size_t(p.nrows) * k * ys;
 	int rc = FMX_OK;
-	gpu_part::async_stage *sg = nullptr;
-	for (gpu_part::async_stage &a : p.async_stages)
-		if (a.st == st) sg = &a;
-	if (!sg) {
-		p.async_stages.push_back(gpu_part::async_stage{st, nullptr, nullptr, 0, 0, nullptr});
-		sg = &p.async_stages.back();
-		if (cudaEventCreateWithFlags(&sg->done, cudaEventDisableTiming) != cudaSuccess)
+	auto ev = [&](cudaEvent_t &e) {
+		if (!rc && !e && cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
 			rc = set_error(FMX_ERR_CUDA, "event creation failed");
+	};
+	auto stm = [&](cudaStream_t &s) {
+		if (!rc && !s && cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess)
+			rc = set_error(FMX_ERR_CUDA, "stream creation failed");
+	};
+	stm(p.h2d_st);
+	stm(p.d2h_st);
+	ev(p.ev_scratch);
+	gpu_part::async_slot &sl = p.aslot[p.anext & 1];
+	ev(sl.x_ready);
+	ev(sl.spmm_done);
+	ev(sl.y_out);
+	if (!rc && (sl.xb < xb || sl.yb < yb)) {
+		// growing: the slot's earlier call must be through first
+		cudaEventSynchronize(sl.spmm_done);
+		cudaEventSynchronize(sl.y_out);
+		auto grow = [&](void *&buf, size_t &have, size_t need) -> int {
+			if (have >= need) return FMX_OK;
+			if (buf) cudaFree(buf);
+			buf = nullptr; have = 0;
+			if (cudaMalloc(&buf, need) != cudaSuccess)
+				return set_error(FMX_ERR_OOM, "cudaMalloc of %zu staging bytes failed", need);
+			have = need;
+			return FMX_OK;
+		};
+		rc = grow(sl.x, sl.xb, xb);
+		if (!rc) rc = grow(sl.y, sl.yb, yb);
 	}
-	if (!rc && !p.ev_scratch && cudaEventCreateWithFlags(&p.ev_scratch, cudaEventDisableTiming) != cudaSuccess)
-		rc = set_error(FMX_ERR_CUDA, "event creation failed");
-	// the stream's earlier calls must be through their copies before the
-	// staging buffers are reused (a stream handle can be recycled)
-	if (!rc && cudaStreamWaitEvent(st, sg->done, 0) != cudaSuccess) rc = set_error(FMX_ERR_CUDA, "stream wait failed");
-	auto grow = [&](void *&buf, size_t &have, size_t need) -> int {
-		if (have >= need) return FMX_OK;
-		if (buf) {
-			cudaStreamSynchronize(st);
-			cudaFree(buf);
-		}
-		buf = nullptr; have = 0;
-		if (cudaMalloc(&buf, need) != cudaSuccess) return set_error(FMX_ERR_OOM, "cudaMalloc of %zu staging bytes failed", need);
-		have = need;
-		return FMX_OK;
-	};
-	if (!rc) rc = grow(sg->x, sg->xb, xb);
-	if (!rc) rc = grow(sg->y, sg->yb, yb);
 	auto copy = [&](void *dst, size_t dpitch, const void *src, size_t spitch, size_t width, size_t rows,
-			cudaMemcpyKind kind) {
-		if (dpitch == width && spitch == width) return cudaMemcpyAsync(dst, src, width * rows, kind, st);
-		return cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, rows, kind, st);
+			cudaMemcpyKind kind, cudaStream_t s) {
+		if (dpitch == width && spitch == width) return cudaMemcpyAsync(dst, src, width * rows, kind, s);
+		return cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, rows, kind, s);
 	};
-	if (!rc && copy(sg->x, k * xs, X_host, ldx * xs, k * xs, p.ncols, cudaMemcpyHostToDevice) != cudaSuccess)
+	auto wait = [&](cudaStream_t s, cudaEvent_t e) {
+		if (!rc && cudaStreamWaitEvent(s, e, 0) != cudaSuccess) rc = set_error(FMX_ERR_CUDA, "stream wait failed");
+	};
+	auto record = [&](cudaEvent_t e, cudaStream_t s) {
+		if (!rc && cudaEventRecord(e, s) != cudaSuccess) rc = set_error(FMX_ERR_CUDA, "event record failed");
+	};
+	// X in, on the copy-in stream, once the slot's last SpMM has read its X
+	wait(p.h2d_st, sl.spmm_done);
+	if (!rc && copy(sl.x, k * xs, X_host, ldx * xs, k * xs, p.ncols, cudaMemcpyHostToDevice, p.h2d_st) != cudaSuccess)
 		rc = set_error(FMX_ERR_CUDA, "copy of X to the device failed");
-	// the SpMMs of calls on different streams share the matrix's scratch:
-	// each waits for the one issued before it
-	if (!rc && cudaStreamWaitEvent(st, p.ev_scratch, 0) != cudaSuccess) rc = set_error(FMX_ERR_CUDA, "stream wait failed");
-	if (!rc) rc = spmm_part(p, x_type, sg->x, k, y_type, sg->y, k, k, nullptr, nullptr, st);
-	if (!rc && cudaEventRecord(p.ev_scratch, st) != cudaSuccess) rc = set_error(FMX_ERR_CUDA, "event record failed");
-	if (!rc && copy(Y_host, ldy * ys, sg->y, k * ys, k * ys, p.nrows, cudaMemcpyDeviceToHost) != cudaSuccess)
+	record(sl.x_ready, p.h2d_st);
+	// the SpMM on the caller's stream: X arrived, the slot's last Y copied
+	// out, and the SpMM issued before this one done (shared scratch)
+	wait(st, sl.x_ready);
+	wait(st, sl.y_out);
+	wait(st, p.ev_scratch);
+	if (!rc) rc = spmm_part(p, x_type, sl.x, k, y_type, sl.y, k, k, nullptr, nullptr, st);
+	record(sl.spmm_done, st);
+	record(p.ev_scratch, st);
+	// Y out, on the copy-out stream; the call ends on the caller's stream
+	// when Y has arrived
+	wait(p.d2h_st, sl.spmm_done);
+	if (!rc && copy(Y_host, ldy * ys, sl.y, k * ys, k * ys, p.nrows, cudaMemcpyDeviceToHost, p.d2h_st) != cudaSuccess)
 		rc = set_error(FMX_ERR_CUDA, "copy of Y to the host failed");
-	if (!rc && cudaEventRecord(sg->done, st) != cudaSuccess) rc = set_error(FMX_ERR_CUDA, "event record failed");
+	record(sl.y_out, p.d2h_st);
+	wait(st, sl.y_out);
+	p.anext++;
 	cudaSetDevice(cur);
 	return rc;
 }

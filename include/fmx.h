@@ -232,19 +232,21 @@ int fmx_spmm_host(const fmx_matrix *m, int x_type, const void *X_host, int64_t l
                   int y_type, void *Y_host, int64_t ldy, int64_t k);
 
 /* Host-buffer SpMM, asynchronous (no counterpart in the reference, whose
- * multiply is synchronous): enqueues on `stream` the copy of X to the device,
- * the SpMM and the copy of Y back, and returns.  X_host and Y_host must stay
- * valid until the stream has reached the end of the call (synchronise the
- * stream or wait on an event recorded after it).  With pinned host memory
- * (cudaHostAlloc, cudaHostRegister) the copies are asynchronous; pageable
- * memory makes them synchronous.  Each stream gets its own device staging
- * for X and Y, kept by the matrix (grow-only) until it is freed, so calls
- * issued alternately on two streams overlap one call's copy of Y with the
- * next call's copy of X (PCIe carries both directions at once).  The SpMMs
- * of these calls run one after another, ordered by an event, because they
- * share the matrix's scratch; they are not ordered against fmx_spmm calls
- * on other streams.  Calls on one matrix from several host threads are
- * serialised by a lock, but their stream order is the caller's to set. */
+ * multiply is synchronous): enqueues the copy of X to the device, the SpMM
+ * and the copy of Y back, and returns.  The call ends on `stream` when Y has
+ * arrived: X_host and Y_host must stay valid until then (synchronise the
+ * stream or wait on an event recorded after the call).  With pinned host
+ * memory (cudaHostAlloc, cudaHostRegister) the copies are asynchronous;
+ * pageable memory makes them synchronous.  The matrix keeps two device
+ * staging slots (grow-only, freed with the matrix) and two streams of its
+ * own: the copies of X run back to back on one and the copies of Y on the
+ * other, while each SpMM runs on `stream`, so calls issued alternately on two
+ * streams overlap one call's copy of Y with the next call's copy of X (PCIe
+ * carries both directions at once).  The SpMMs of these calls run one after
+ * another, ordered by an event, because they share the matrix's scratch;
+ * they are not ordered against fmx_spmm calls on other streams.  Calls on
+ * one matrix from several host threads are serialised by a lock, but their
+ * stream order is the caller's to set. */
 int fmx_spmm_host_async(const fmx_matrix *m, int x_type, const void *X_host, int64_t ldx,
                         int y_type, void *Y_host, int64_t ldy, int64_t k, void *stream);
 
