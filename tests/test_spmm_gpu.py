@@ -259,8 +259,9 @@ def test_host_buffers_e2e(torch_cuda):
 
 def test_host_buffers_async_two_streams(torch_cuda):
     """fmx_spmm_host_async: six calls in flight on two streams, each with its
-    own pinned X and Y; every Y equals the oracle's (integer-valued X, so
-    exact), and a recycled stream reuses its staging."""
+    own pinned X and Y, through the matrix's two staging slots; every Y equals
+    the oracle's (integer-valued X, so exact), and so does a later call on a
+    third stream."""
     torch = torch_cuda
     src, dst = _graph(20000, 100000, 23, ((7, 15000), (11, 900)))
     idx, mat = oracle.build_image(src, dst, None, block=(4096, 4096), dedup=True)
