@@ -58,6 +58,8 @@ def test_status_strings():
 def test_null_arguments_are_rejected():
     assert _lib.lib.fmx_matrix_create(None, None, 0, None) == _lib.FMX_ERR_INVAL
     assert _lib.lib.fmx_spmm(None, 0, None, 1, 0, None, 1, 1, None, None, None) == _lib.FMX_ERR_INVAL
+    assert _lib.lib.fmx_spmm_host(None, 0, None, 1, 0, None, 1, 1) == _lib.FMX_ERR_INVAL
+    assert _lib.lib.fmx_spmm_host_async(None, 0, None, 1, 0, None, 1, 1, None) == _lib.FMX_ERR_INVAL
     assert _lib.lib.fmx_image_free(None) == _lib.FMX_OK
     assert _lib.lib.fmx_matrix_free(None) == _lib.FMX_OK
 
