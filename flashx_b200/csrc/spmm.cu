@@ -46,12 +46,15 @@
 // before it).  Every row of up to kExactMax entries is summed by one group in
 // the reference's order (bit-identical results).  No atomics: every output
 // row is written exactly once.  Three row kernels share that scheme:
-//   spmm_wide_kernel  FP32 panels of 32, 64 or 128 bytes: a lane owns 32 bytes
-//                     of each gathered row; 8 column ids per 32-byte load
-//   spmm_kernel       16-byte lanes (BF16, FP64, integer and odd widths),
-//                     with L2 evict_last hints on hot-pack gathers and
-//                     evict_first on cold rows
+//   spmm_wide_kernel  FP32 panels of 32, 64 or 128 bytes, and unweighted BF16
+//                     into BF16: a lane owns 32 bytes of each gathered row;
+//                     8 column ids per 32-byte load
+//   spmm_kernel       16-byte lanes (BF16 into FP32, weighted BF16, FP64,
+//                     integer and odd widths), with L2 evict_last hints on
+//                     hot-pack gathers and evict_first on cold rows
 //   spmv_kernel       k = 1: a warp per range, gathers staged in shared memory
+// Each call first packs the hot rows: pack_hot_vec_kernel in 16-byte units,
+// pack_hot_kernel one element per thread (k = 1 and rows of odd widths).
 #include "fmx_internal.h"
 
 #include <cuda_runtime.h>
